@@ -1,0 +1,414 @@
+"""Benchmark of the GPU grouped aggregate (one JSON line on stdout, rank 0).
+
+Default workload: the low-cardinality decimal report aggregate (60M rows,
+two dictionary keys -> 6 groups, four DECIMAL(12,2) columns; sum(qty),
+sum(price), sum(price*(1-disc)), sum(price*(1-disc)*(1+tax)) in exact
+decimal, avg(qty), avg(disc), count(*)) -- the TPC-H Q1 shape the reference
+quotes its headline numbers on. A step is one pass of the aggregate over the
+whole input: table clear + aggregate kernel, inputs resident in HBM (2.4 GB,
+larger than the 126 MB L2). `e2e` is the same work through the public C ABI
+with pinned host buffers: H2D of the step's inputs (chunked, copies
+overlapping kernels) + the emitted groups copied back.
+
+Other workloads (--workload plain|highcard|batched|serving) print the same
+line for their own shape. --impl reference times the CPU port of the
+reference's aggregate (oracle/) on the host cores instead.
+
+Multi-GPU (torchrun): every rank aggregates its own replica of the workload
+(weak scaling, no collective on the data path); time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "rows/s & HBM GB/s (% of peak), batched vs plain on 1 B200; serving p50/p99 ms"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm = []
+        mx = None
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except (ValueError, IndexError):
+                continue
+            for name, val in zip(names, r[5:9]):
+                if val.strip().lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ workloads
+def make_workload(name, rows=None):
+    from vecruntime_b200 import datagen as G
+
+    if name == "decimal":
+        return G.decimal_report(rows=rows or 60_000_000)
+    if name == "plain":
+        return G.plain(rows=rows or (1 << 20))
+    if name == "highcard":
+        return G.high_cardinality(rows=rows or 100_000_000)
+    raise ValueError(name)
+
+
+def output_row_bytes(types):
+    b = 0.0
+    for t in types:
+        b += {1: 4, 2: 8, 3: 8, 4: 0.125, 5: 16, 6: 4}[t.lane] + 0.125
+    return b
+
+
+def device_batch(w, device):
+    import torch
+
+    from vecruntime_b200 import columns as Cc
+
+    db, tensors = Cc.to_device(w.batch(), device)
+    torch.cuda.synchronize(device)
+    return db, tensors
+
+
+def pinned_copy(w, lib):
+    """The workload's columns copied into pinned host memory (vr_host_alloc)."""
+    from vecruntime_b200 import columns as Cc
+
+    bufs = []
+
+    def pin(a):
+        if a is None:
+            return None
+        a = np.ascontiguousarray(a)
+        p = C.c_void_p()
+        rc = lib.vr_host_alloc(max(a.nbytes, 16), C.byref(p))
+        assert rc == 0, "pinned allocation"
+        dst = np.ctypeslib.as_array((C.c_uint8 * a.nbytes).from_address(p.value)).view(a.dtype).reshape(a.shape)
+        dst[...] = a
+        bufs.append(p)
+        return dst
+
+    cols = []
+    for c in w.columns:
+        n = Cc.Col(c.lane, pin(c.data), pin(c.validity), c.precision, c.scale, c.dict_size, c.nullable)
+        if c.lane == 4:
+            n._n = c._n
+        cols.append(n)
+    return cols, bufs
+
+
+def cpu_baseline(w, sample_rows, threads):
+    from oracle import pyoracle as O
+    from vecruntime_b200 import datagen as G
+
+    sub = G.Workload(w.name, w.columns, w.keys, w.functions, w.est_groups, w.rows)
+    batch = sub.batch(0, sample_rows)
+    secs, groups = O.run_threads(w.spec(), batch, threads, 4096)
+    return sample_rows / secs, secs
+
+
+# ------------------------------------------------------------------ our arm
+def run_ours(args, rank, world, device):
+    import torch
+
+    import vecruntime_b200 as vr
+    from vecruntime_b200 import native as N
+
+    torch.cuda.set_device(device)
+    lib = N.lib()
+    w = make_workload(args.workload, args.rows)
+    log(f"[rank {rank}] workload {w.name}: {w.rows} rows, est groups {w.est_groups}")
+    db, tensors = device_batch(w, device)
+    agg = vr.GpuHashAggregate(w.columns, w.keys, w.functions, est_groups=w.est_groups, max_batch_rows=w.rows,
+                              device=device, flags=N.VR_SPEC_TRACE)
+    stream = torch.cuda.ExternalStream(agg.stream(), device=torch.device("cuda", device))
+    # warm-up
+    for _ in range(args.warmup):
+        agg.reset()
+        agg.consume(db)
+        agg.sync()
+    groups = agg.num_groups()
+    st0 = agg.stats()
+    kms0 = st0.total_kernel_ms
+    launches0 = st0.kernel_launches
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    dist_barrier(world)
+    torch.cuda.synchronize(device)
+    with ClockSampler(device) as clocks:
+        for i in range(args.steps):
+            ev[i][0].record(stream)
+            agg.reset()
+            agg.consume(db)
+            ev[i][1].record(stream)
+            agg.sync()
+        torch.cuda.synchronize(device)
+    dist_barrier(world)
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    st1 = agg.stats()
+    kernel_ms = (st1.total_kernel_ms - kms0) / args.steps
+    launches = st1.kernel_launches - launches0
+    total_ms = sum(step_ms)
+    total_ms = dist_max(total_ms, world, device)
+    ms_per_step = total_ms / args.steps
+    rows_total = w.rows * world
+    value = rows_total / (ms_per_step * 1e-3)
+
+    from vecruntime_b200 import datagen as G
+
+    out_types = agg.output_types
+    in_bytes = G.input_bytes(w)
+    out_bytes = groups * output_row_bytes(out_types)
+    alg_bytes = in_bytes + out_bytes
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / (kernel_ms * 1e-3) / 1e9
+    agg.close()
+    del tensors
+
+    # end to end through the public API: pinned host buffers, H2D + D2H in the step
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(args, w, lib, device, out_types)
+        if e2e is not None:
+            e2e["value"] = dist_min(e2e["value"], world, device) * world
+
+    result = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "rows/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_per_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "int64 (exact decimal128 sums)" if w.name == "decimal" else "int64/f64",
+        "data": "synthetic (seeded; shapes of the workload, no benchmark data reproduced)",
+        "config": {"workload": workload_label(w), "rows_per_gpu": w.rows, "groups": groups,
+                   "batch": "one device-resident batch per step",
+                   "l2": "inputs larger than L2 (%.2f GB > 126 MB)" % (in_bytes / 1e9),
+                   "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "algorithmic_bytes_per_launch": alg_bytes, "kernel_ms": kernel_ms},
+        "e2e": e2e,
+        "gpu_launches": launches,
+        "clocks": clocks.summary(),
+    }
+    return result, w
+
+
+def workload_label(w):
+    return {"decimal": "low-cardinality decimal report: 60M rows, 2 dictionary keys (3x2 -> 6 groups), "
+                       "4 DECIMAL(12,2) columns, exact decimal(38,6) sums",
+            "plain": "plain grouped aggregation: 1,048,576 rows, int64 key over 1,000 values, 5% nulls",
+            "highcard": "high-cardinality composite key: 100M rows, Zipf(1.1) int64 x int32[16], 1% null keys"
+            }.get(w.name, w.name)
+
+
+def run_e2e(args, w, lib, device, out_types):
+    import torch
+
+    import vecruntime_b200 as vr
+    from vecruntime_b200 import columns as Cc
+    from vecruntime_b200 import datagen as G
+    from vecruntime_b200 import native as N
+
+    cols, bufs = pinned_copy(w, lib)
+    chunk = min(w.rows, args.chunk_rows)
+    chunk -= chunk % 128 if chunk > 128 else 0
+    agg = vr.GpuHashAggregate(w.columns, w.keys, w.functions, est_groups=w.est_groups, max_batch_rows=chunk,
+                              device=device)
+    stream = torch.cuda.ExternalStream(agg.stream(), device=torch.device("cuda", device))
+
+    def batches():
+        out = []
+        for lo in range(0, w.rows, chunk):
+            hi = min(w.rows, lo + chunk)
+            out.append(Cc.HostBatch([G.slice_col(c, lo, hi) for c in cols], hi - lo))
+        return out
+
+    bl = batches()
+    groups = 0
+    in_bytes = G.input_bytes(w)
+    d2h = 0
+    times = []
+    for it in range(args.warmup + args.steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        agg.reset()
+        for hb in bl:
+            agg.consume(hb)
+        groups = agg.num_groups()
+        out = agg.emit()
+        b.record(stream)
+        torch.cuda.synchronize(device)
+        if it >= args.warmup:
+            times.append(a.elapsed_time(b))
+        d2h = sum(d.nbytes + v.nbytes for d, v in out)
+    agg.close()
+    for p in bufs:
+        lib.vr_host_free(p)
+    ms = float(np.mean(times))
+    return {"value": w.rows / (ms * 1e-3), "unit": "rows/s", "h2d_bytes_per_step": in_bytes,
+            "d2h_bytes_per_step": d2h, "ms_per_step": ms, "chunk_rows": chunk}
+
+
+# ------------------------------------------------------------------ reference arm
+def run_reference(args):
+    """The CPU port of the reference's aggregate (oracle/) on the host cores:
+    bounded samples of the same workload, every host thread."""
+    threads = os.cpu_count() or 1
+    w = make_workload(args.workload, args.rows)
+    sample = min(w.rows, args.cpu_sample_rows)
+    for _ in range(args.warmup):
+        cpu_baseline(w, min(sample, 1 << 20), threads)
+    rates = []
+    for _ in range(args.steps):
+        r, secs = cpu_baseline(w, sample, threads)
+        rates.append(r)
+    value = float(np.median(rates))
+    return {
+        "metric": METRIC, "impl": "reference", "value": value, "unit": "rows/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": w.rows / value * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64 (exact decimal128 sums)",
+        "data": "synthetic (seeded)", "config": {"workload": workload_label(w), "rows_per_gpu": w.rows},
+        "cpu_baseline": {"value": value, "unit": "rows/s", "cores": threads, "kind": "port",
+                         "sample": f"{sample} of {w.rows} rows per step, {threads} threads (one partition each, "
+                                   f"4096-row batches, partitions merged)"},
+        "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+# ------------------------------------------------------------------ distributed
+def dist_barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def dist_max(x, world, device):
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device=torch.device("cuda", device))
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_min(x, world, device):
+    return -dist_max(-x, world, device)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="decimal", choices=["decimal", "plain", "highcard"])
+    ap.add_argument("--rows", type=int, default=None)
+    ap.add_argument("--chunk-rows", type=int, default=8 << 20)
+    ap.add_argument("--cpu-sample-rows", type=int, default=8_000_000)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return
+
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    result, w = run_ours(args, rank, world, local)
+    if rank == 0 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        sample = min(w.rows, args.cpu_sample_rows)
+        rate, secs = cpu_baseline(w, sample, threads)
+        result["cpu_baseline"] = {"value": rate, "unit": "rows/s", "cores": threads, "kind": "port",
+                                  "sample": f"{sample} of {w.rows} rows, {threads} threads, {secs:.2f} s"}
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,369 @@
+/*
+ * vrgpu.h -- C ABI of the B200 grouped-aggregation backend (libvrgpu.so).
+ *
+ * One hot path: partial and final grouped aggregation over Arrow-layout
+ * batches (key hashing, group probe/insert into an open-addressing table,
+ * count/sum/min/max/avg that honour validity bitmaps, exact 128-bit decimal
+ * sums with Spark's null and overflow rules).
+ *
+ * The entry points replace the kernel-level contract of the reference's
+ * aggregate operator (vecruntime, Java):
+ *   GroupKeyTable.assign(keys, n, outIds, selection)
+ *       kernels/src/main/java/io/vecruntime/kernels/GroupKeyTable.java:709-764
+ *   GroupedAccumulators.*.update(v, assignment)
+ *       kernels/src/main/java/io/vecruntime/kernels/GroupedAccumulators.java:195-1462
+ *   GroupKeyTable.writeKeys / GroupedAggState.writeBuffer (emission)
+ *       kernels/src/main/java/io/vecruntime/kernels/GroupKeyTable.java:2851-2920
+ *       spark/src/main/scala/io/vecruntime/spark/agg/VectorAggregates.scala:54-97
+ * as driven by VectorGroupedAggregateIterator.consume / buildBatch
+ *       spark/src/main/scala/org/apache/spark/sql/vecruntime/VectorHashAggregateExec.scala:584-602, 831-913
+ *
+ * Conventions
+ *   - Every call returns a status code (VR_OK = 0); nothing throws across
+ *     the boundary. After an error other than VR_ERR_INVALID /
+ *     VR_ERR_UNSUPPORTED the handle is dead: the caller destroys it (the
+ *     Java side closes it, as the reference's task-completion listener does).
+ *   - One handle per task thread; a handle is not thread-safe. Many handles
+ *     run concurrently, each on its own CUDA stream.
+ *   - Buffers are Arrow layout: little-endian values, LSB-first validity
+ *     bitmaps starting at bit 0 (NULL = every row valid), DECIMAL128 as two
+ *     little-endian int64 limbs (lo at 16*i, hi at 16*i+8), BOOL as a packed
+ *     bitmap.
+ *   - The caller owns input buffers and keeps them alive (and, for async
+ *     copies, pinned: vr_host_alloc / vr_host_register) until vr_agg_sync
+ *     returns. The caller owns output buffers. The handle owns device state.
+ */
+#ifndef VRGPU_H
+#define VRGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VRGPU_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+enum vr_status {
+    VR_OK = 0,
+    VR_ERR_INVALID = 1,           /* bad argument or spec                        */
+    VR_ERR_OOM = 2,               /* device or pinned allocation refused         */
+    VR_ERR_OVERFLOW = 3,          /* ANSI bigint sum overflow: Spark's
+                                     ARITHMETIC_OVERFLOW (VectorAggregates.scala:145-146) */
+    VR_ERR_DECIMAL_PRECISION = 4, /* ANSI decimal result past its precision
+                                     (VectorAggregates.scala:333-341)            */
+    VR_ERR_TIMEOUT = 5,           /* a bounded device wait gave up               */
+    VR_ERR_CUDA = 6,              /* CUDA runtime error; text in vr_agg_last_error */
+    VR_ERR_UNSUPPORTED = 7,       /* outside the GPU gate: caller falls back to
+                                     the Vector API path, then Spark             */
+    VR_ERR_STATE = 8,             /* dead handle or call out of order            */
+    VR_ERR_ADMISSION = 9,         /* serving: request larger than the HBM cap    */
+    VR_ERR_DECIMAL_OVERFLOW = 10  /* ANSI overflow of a merged decimal sum:
+                                     Spark's overflowInSumOfDecimal (VectorAggregates.scala:737-741) */
+};
+
+/* ---- lane types (reference VecType, kernels/.../VecType.java:23-64) ---- */
+enum vr_lane {
+    VR_INT32 = 1,
+    VR_INT64 = 2,      /* also DECIMAL(p<=18, s) unscaled (TypeMapping.java:87-90) */
+    VR_FLOAT64 = 3,    /* keys group by raw bits (GroupKeyTable.java:2350-2353)    */
+    VR_BOOL = 4,       /* bit-packed                                               */
+    VR_DECIMAL128 = 5, /* DECIMAL(p>18, s): two LE int64 limbs (Decimal128.java:21-61) */
+    VR_DICT32 = 6      /* UTF8 key as a dictionary id (int32); GroupKeyTable keeps
+                          strings as ids (GroupKeyTable.java:27-36)                */
+};
+
+typedef struct vr_column_type {
+    int32_t lane;      /* enum vr_lane                                          */
+    int32_t precision; /* decimal precision; 0 when not a decimal               */
+    int32_t scale;     /* decimal scale                                         */
+    int32_t nullable;  /* 0: the column never carries a validity bitmap         */
+    int32_t dict_size; /* VR_DICT32 / VR_BOOL keys: ids lie in [0, dict_size);
+                          0 = unknown (no direct indexing)                      */
+    int32_t reserved;
+} vr_column_type;
+
+/* ---- aggregate functions (reference VectorAggFunction implementations) -- */
+enum vr_fn_kind {
+    VR_FN_COUNT_STAR = 1,      /* CountAgg(None)           VectorAggregates.scala:906-926  */
+    VR_FN_COUNT = 2,           /* CountAgg(Some(e))                                        */
+    VR_FN_SUM_LONG = 3,        /* SumLongAgg (INT32/INT64) VectorAggregates.scala:142-200  */
+    VR_FN_SUM_DOUBLE = 4,      /* SumDoubleAgg             VectorAggregates.scala:118-136  */
+    VR_FN_AVG_DOUBLE = 5,      /* AverageAgg (sum, count)  VectorAggregates.scala:1021-1039 */
+    VR_FN_MIN = 6,             /* MinMaxAgg(isMin = true)  VectorAggregates.scala:929-1018 */
+    VR_FN_MAX = 7,             /* MinMaxAgg(isMin = false)                                 */
+    VR_FN_SUM_DECIMAL = 8,     /* WideDecimalSumAgg (sum, isEmpty) VectorAggregates.scala:318-395 */
+    VR_FN_AVG_DECIMAL = 9,     /* WideDecimalAvgAgg (sum, count)   VectorAggregates.scala:444-516 */
+    VR_FN_COUNT_MERGE = 10,    /* CountMergeAgg            VectorAggregates.scala:1042-1059 */
+    VR_FN_AVG_DOUBLE_MERGE = 11,  /* AverageMergeAgg       VectorAggregates.scala:1065-1090 */
+    VR_FN_SUM_DECIMAL_MERGE = 12, /* WideDecimalSumMergeAgg VectorAggregates.scala:658-781  */
+    VR_FN_AVG_DECIMAL_MERGE = 13  /* WideDecimalAvgMergeAgg VectorAggregates.scala:526-642  */
+};
+/* A merge of SumLong / SumDouble / MinMax buffers is VR_FN_SUM_LONG /
+ * VR_FN_SUM_DOUBLE / VR_FN_MIN / VR_FN_MAX over the buffer column, exactly as
+ * compileMerge builds them (VectorAggregates.scala:1197-1215). */
+
+enum vr_fn_flags {
+    VR_FN_CHECKED = 1,          /* ANSI bigint sum: overflow -> VR_ERR_OVERFLOW      */
+    VR_FN_NULL_ON_OVERFLOW = 2, /* non-ANSI decimal: past precision -> null          */
+    VR_FN_FINAL = 4,            /* Final / Complete result in the sum slot           */
+    VR_FN_STRICT = 8            /* accepted for parity with spark.vecruntime.exec.strictFloatingPoint;
+                                   FP64 sums are compensated, not sequential          */
+};
+
+/* One factor of a fused decimal product: value = addend + sign * column,
+ * unscaled at the column's scale (e.g. (1 - disc) with disc DECIMAL(12,2):
+ * addend 100, sign -1). Replaces the reference's SpeculativeDecimalMulExpr
+ * (spark/.../expr/DecimalExprs.scala:470-516) in front of a decimal sum. */
+typedef struct vr_term {
+    int32_t column;
+    int32_t sign; /* +1 or -1 */
+    int64_t addend;
+} vr_term;
+
+typedef struct vr_agg_fn {
+    int32_t kind;      /* enum vr_fn_kind                                         */
+    int32_t input;     /* input column (-1 for COUNT_STAR); merges: 1st buffer col */
+    int32_t input2;    /* merges: 2nd buffer column (count / isEmpty); else -1     */
+    int32_t flags;     /* enum vr_fn_flags                                         */
+    int32_t precision; /* decimal sum/avg buffer type (Spark: Decimal(p + 10, s))  */
+    int32_t scale;
+    int32_t num_terms; /* 0: input column; 2..3: exact product of terms[]          */
+    int32_t product_precision; /* declared precision of the product (0 = 38): a row
+                                  whose exact product reaches 10^p is null (non-ANSI)
+                                  or VR_ERR_DECIMAL_PRECISION with VR_FN_CHECKED,
+                                  Spark's CheckOverflow on the multiply            */
+    vr_term terms[3];
+} vr_agg_fn;
+
+enum vr_spec_flags {
+    VR_SPEC_FORCE_GLOBAL = 1,  /* tests / tuning: skip the shared-memory tiers   */
+    VR_SPEC_FORCE_SHARED = 2,  /* shared-memory hash table in front of HBM       */
+    VR_SPEC_FORCE_DIRECT = 4,  /* direct-indexed thread-private tier             */
+    VR_SPEC_NO_WARP_AGG = 8,   /* no __match_any_sync pre-aggregation            */
+    VR_SPEC_WARP_AGG = 16,     /* force __match_any_sync pre-aggregation         */
+    VR_SPEC_NO_TMA = 32,       /* plain loads instead of bulk copies into smem   */
+    VR_SPEC_TRACE = 64         /* record cudaEvent pairs per H2D / kernel / D2H  */
+};
+
+typedef struct vr_agg_spec {
+    int32_t num_columns;            /* input columns per batch                 */
+    const vr_column_type* columns;
+    int32_t num_keys;               /* 0 = ungrouped (one group)               */
+    const int32_t* key_columns;
+    int32_t num_fns;
+    const vr_agg_fn* fns;
+    int64_t est_groups;             /* cardinality estimate; 0 = unknown       */
+    int64_t max_batch_rows;         /* largest host batch (device staging)     */
+    int32_t device;                 /* CUDA device ordinal                     */
+    int32_t flags;                  /* enum vr_spec_flags                      */
+} vr_agg_spec;
+
+/* ---- batches ----------------------------------------------------------- */
+enum vr_location { VR_HOST = 0, VR_DEVICE = 1 };
+
+typedef struct vr_column {
+    const void* data;
+    const uint8_t* validity; /* NULL = all valid */
+} vr_column;
+
+typedef struct vr_batch {
+    int64_t num_rows;
+    const vr_column* columns;  /* spec->num_columns entries                    */
+    const uint8_t* selection;  /* NULL = every row; unselected rows never
+                                  create a group (GroupKeyTable.java:705-708)   */
+    int32_t location;          /* enum vr_location                             */
+    int32_t reserved;
+} vr_batch;
+
+typedef struct vr_out_column {
+    void* data;
+    uint8_t* validity;         /* ceil(n/8) bytes; written for every row       */
+} vr_out_column;
+
+typedef struct vr_agg_stats {
+    int32_t tier;              /* 0 direct, 1 shared+global, 2 global           */
+    int32_t warp_agg;          /* 1 when __match_any_sync pre-aggregation is on */
+    int64_t table_capacity;    /* global slots                                  */
+    int64_t slot_bytes;
+    int64_t groups;            /* after the last sync                           */
+    int64_t rows;              /* rows consumed                                 */
+    int64_t batches;
+    int64_t rehashes;
+    int64_t deferred_rows;     /* rows replayed after a table grow              */
+    int32_t threads;           /* per block                                     */
+    int32_t blocks;            /* per launch                                    */
+    int32_t smem_bytes;
+    int32_t tile_rows;
+    double last_kernel_ms;     /* VR_SPEC_TRACE only                            */
+    double total_kernel_ms;
+    double total_h2d_ms;
+    double total_d2h_ms;
+    int64_t kernel_launches;   /* every kernel this handle launched             */
+} vr_agg_stats;
+
+typedef struct vr_agg vr_agg;
+
+/* ---- lifecycle ----------------------------------------------------------
+ * vr_agg_create: GroupKeyTable + GroupedAggState construction
+ *   (VectorAggFunction.newGroupedState, VectorAggregates.scala:100-111;
+ *    GroupKeyTable constructor, GroupKeyTable.java:563-600). Returns
+ *   VR_ERR_UNSUPPORTED for specs outside the GPU gate. */
+int vr_agg_create(const vr_agg_spec* spec, vr_agg** out);
+
+/* vr_agg_update: GroupKeyTable.assign + GroupedAggState.update for one batch
+ *   (GroupKeyTable.java:709-764; VectorAggregates.scala:54-55;
+ *    VectorHashAggregateExec.scala:584-602). Asynchronous on the handle's
+ *   stream; host inputs are copied to HBM first. */
+int vr_agg_update(vr_agg* h, const vr_batch* batch);
+
+/* Waits for every queued update; surfaces device-side errors. */
+int vr_agg_sync(vr_agg* h);
+
+/* GroupKeyTable.size() (GroupKeyTable.java:683, the value assign returns at :709-764). Syncs. */
+int vr_agg_num_groups(vr_agg* h, int64_t* groups);
+
+/* Output columns: the keys, then each function's Spark buffer slots
+ *   (VectorAggFunction.bufferTypes / emittedTypes, VectorAggregates.scala:100-111). */
+int vr_agg_output_schema(const vr_agg* h, int32_t* num_out, vr_column_type* types, int32_t cap);
+
+/* vr_agg_emit: groups [from, to) as Arrow columns into caller buffers
+ *   (GroupKeyTable.writeKeys GroupKeyTable.java:2851-2920;
+ *    GroupedAggState.writeBuffer VectorAggregates.scala:62, 179-198, 374-389;
+ *    VectorGroupedAggregateIterator.buildBatch VectorHashAggregateExec.scala:831-913).
+ *   Group order is the table's slot order (stable until the next update).
+ *   `location` says where the output buffers live. */
+int vr_agg_emit(vr_agg* h, int64_t from, int64_t to, const vr_out_column* outs, int32_t location);
+
+/* Empties the table, keeping its memory (EmitAndReset,
+ *   VectorHashAggregateExec.scala:193-246). */
+int vr_agg_reset(vr_agg* h);
+
+/* Frees device state (GroupedAggState.close, VectorAggregates.scala:85-90). */
+void vr_agg_destroy(vr_agg* h);
+
+int vr_agg_get_stats(const vr_agg* h, vr_agg_stats* stats);
+int vr_agg_last_error(const vr_agg* h, char* buf, size_t cap);
+const char* vr_status_string(int status);
+/* The message of the last failed vr_agg_create / vr_srv_* on this thread. */
+const char* vr_thread_last_error(void);
+/* The CUDA stream the handle launches on (cudaStream_t), for event timing. */
+void* vr_agg_stream(const vr_agg* h);
+
+/* ---- pinned host memory (the GPU analogue of NativePool, NativePool.java:76-87) */
+int vr_host_alloc(size_t bytes, void** out);
+int vr_host_free(void* p);
+int vr_host_register(void* p, size_t bytes);
+int vr_host_unregister(void* p);
+
+/* ---- row hash parity (HashKernels.init/mixColumn/finish,
+ *      kernels/.../HashKernels.java:42-236). Device pointers; out[n]. ------ */
+int vr_hash_rows(int32_t num_keys, const vr_column_type* types, const vr_column* keys,
+                 int64_t num_rows, uint32_t* out_device, int32_t finish, void* stream);
+
+/* ---- batched persistent aggregation ------------------------------------
+ * Many independent instances (Spark tasks' batches) in one persistent
+ * launch, optionally replayed from a CUDA graph. No reference analogue:
+ * the reference runs one task per thread (VectorHashAggregateExec.scala:248-302). */
+enum vr_batched_mode { VR_BATCHED_PERSISTENT = 0, VR_BATCHED_PLAIN = 1 };
+
+typedef struct vr_batched_plan {
+    int32_t num_instances;
+    vr_agg* const* instances;  /* handles created on the same device          */
+    const vr_batch* batches;   /* one device-resident batch per instance     */
+    int32_t mode;              /* enum vr_batched_mode                        */
+    int32_t use_graph;         /* capture once, replay on later calls         */
+} vr_batched_plan;
+
+typedef struct vr_batched vr_batched;
+int vr_batched_create(const vr_batched_plan* plan, vr_batched** out);
+/* Resets every instance's table, then aggregates every instance's batch. */
+int vr_batched_run(vr_batched* b, void* stream);
+void vr_batched_destroy(vr_batched* b);
+
+/* ---- autotuner (table size, block shape, tier) keyed on rows and
+ *      estimated cardinality ------------------------------------------- */
+typedef struct vr_tune_choice {
+    int32_t tier;           /* 0 direct, 1 shared cache + HBM, 2 HBM only           */
+    int32_t warp_agg;       /* __match_any_sync pre-aggregation                     */
+    int32_t threads;        /* consumer threads per block (0 = default)             */
+    int32_t blocks_per_sm;  /* 0 = default                                          */
+    int32_t tile_rows;      /* rows per staged tile, multiple of 128 (0 = default)  */
+    int32_t smem_slots;     /* shared cache slots, power of two (0 = default)       */
+    int64_t table_capacity; /* HBM slots, power of two (0 = from est_groups)        */
+} vr_tune_choice;
+/* vr_agg_create with a forced configuration (tests, the tuner's search). */
+int vr_agg_create_tuned(const vr_agg_spec* spec, const vr_tune_choice* choice, vr_agg** out);
+/* Runs every candidate configuration on one device-resident batch, times it
+ * with CUDA events and records the fastest for (spec, rows, est_groups). */
+int vr_tune_search(const vr_agg_spec* spec, const vr_batch* device_batch, int32_t iters, vr_tune_choice* best,
+                   double* best_rows_per_s);
+
+/* ---- plan inspection (host only; no GPU needed) ------------------------ */
+typedef struct vr_plan_info {
+    int32_t key_words;      /* packed key words per slot                           */
+    int32_t acc_words;      /* accumulator words per slot                          */
+    int32_t slot_words;
+    int32_t num_ops;
+    int32_t num_outputs;
+    int32_t staged_columns;
+    int32_t sentinel_layout;/* single 64-bit key stored xor a constant             */
+    int32_t direct_ok;      /* dictionary / boolean keys: dense combination space  */
+    int64_t direct_slots;
+    char reason[160];       /* why a spec was refused                              */
+} vr_plan_info;
+int vr_agg_plan(const vr_agg_spec* spec, vr_plan_info* info, vr_column_type* out_types, int32_t cap);
+/* 1 and the recorded choice when the tuner has one for (spec, rows), else 0. */
+int vr_tune_lookup(const vr_agg_spec* spec, int64_t rows, vr_tune_choice* out);
+int vr_tune_record(const vr_agg_spec* spec, int64_t rows, const vr_tune_choice* choice, double rows_per_s);
+int vr_tune_load(const char* path);
+int vr_tune_save(const char* path);
+
+/* ---- serving: continuous batching over resident per-query tables ------- */
+typedef struct vr_srv_config {
+    int32_t device;
+    int32_t slots;             /* concurrent requests on the device           */
+    int64_t hbm_cap_bytes;     /* admission cap for staging + tables          */
+    int64_t staging_bytes_per_slot;
+    int32_t flags;
+    int32_t reserved;
+} vr_srv_config;
+
+typedef struct vr_srv_stats {
+    int64_t submitted;
+    int64_t completed;
+    int64_t admitted_immediately;
+    int64_t queued;            /* waited for a slot or for memory              */
+    int64_t rejected;
+    int64_t rows;
+    double p50_ms;             /* submit -> result ready                       */
+    double p99_ms;
+    double max_ms;
+    double mean_ms;
+    int64_t hbm_in_use;
+    int64_t hbm_peak;
+} vr_srv_stats;
+
+typedef struct vr_srv vr_srv;
+int vr_srv_create(const vr_srv_config* cfg, vr_srv** out);
+/* Opens a live query whose table stays resident in HBM. */
+int vr_srv_open_query(vr_srv* s, const vr_agg_spec* spec, int32_t* query_id);
+/* Queues one partial-aggregation batch (host memory, pinned for overlap).
+ * The caller keeps the batch's buffers alive until the ticket completes. */
+int vr_srv_submit(vr_srv* s, int32_t query_id, const vr_batch* batch, uint64_t* ticket);
+/* Waits for a ticket; latency is submit -> device completion. */
+int vr_srv_wait(vr_srv* s, uint64_t ticket, double* latency_ms);
+/* Waits for every queued request of the query, then exposes its handle
+ * for vr_agg_num_groups / vr_agg_emit. The server keeps ownership. */
+int vr_srv_query_handle(vr_srv* s, int32_t query_id, vr_agg** h);
+int vr_srv_close_query(vr_srv* s, int32_t query_id);
+int vr_srv_get_stats(vr_srv* s, vr_srv_stats* st);
+int vr_srv_drain(vr_srv* s);
+void vr_srv_destroy(vr_srv* s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VRGPU_H */

@@ -1,0 +1,133 @@
+"""ctypes binding of the CPU oracle (oracle/_build/liborc.so).
+
+TEST INFRASTRUCTURE ONLY: tests/, __graft_entry__.smoke() and bench.py's
+CPU-baseline leg use it as the checker / the timed CPU port; the product
+path never does. Shares only the ABI structs (include/vrgpu.h) with it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from vecruntime_b200 import native as N
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "liborc.so")
+
+ORC_FP_SEQUENTIAL = 0
+ORC_FP_COMPENSATED = 1
+
+_lib = None
+
+
+def build() -> None:
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        P = C.c_void_p
+        L.orc_agg_create.argtypes = [C.POINTER(N.AggSpec), C.POINTER(P)]
+        L.orc_agg_update.argtypes = [P, C.POINTER(N.Batch), C.c_int64]
+        L.orc_agg_num_groups.argtypes = [P]
+        L.orc_agg_num_groups.restype = C.c_int64
+        L.orc_agg_num_outputs.argtypes = [P]
+        L.orc_agg_output_type.argtypes = [P, C.c_int, C.POINTER(N.ColumnType)]
+        L.orc_agg_emit.argtypes = [P, C.c_int64, C.c_int64, C.POINTER(N.OutColumn), C.c_int]
+        L.orc_agg_merge.argtypes = [P, P]
+        L.orc_agg_destroy.argtypes = [P]
+        L.orc_agg_destroy.restype = None
+        L.orc_last_error.restype = C.c_char_p
+        L.orc_hash_rows.argtypes = [C.c_int32, C.POINTER(N.ColumnType), C.POINTER(N.Column), C.c_int64, P, C.c_int32]
+        L.orc_agg_run_threads.argtypes = [C.POINTER(N.AggSpec), C.POINTER(N.Batch), C.c_int32, C.c_int64,
+                                          C.POINTER(C.c_double), C.POINTER(C.c_int64)]
+        _lib = L
+    return _lib
+
+
+class OracleError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"oracle: {msg} (status {status})")
+        self.status = status
+
+
+class Oracle:
+    """The reference's grouped aggregate restated on the CPU (first-seen group order)."""
+
+    def __init__(self, spec):
+        self.spec = spec  # vecruntime_b200.aggregate.Spec (keeps arrays alive)
+        self.h = C.c_void_p()
+        rc = lib().orc_agg_create(C.byref(spec.spec), C.byref(self.h))
+        if rc:
+            raise OracleError(rc, lib().orc_last_error().decode())
+        n = lib().orc_agg_num_outputs(self.h)
+        self.output_types = []
+        for i in range(n):
+            t = N.ColumnType()
+            lib().orc_agg_output_type(self.h, i, C.byref(t))
+            self.output_types.append(t)
+
+    def update(self, batch, chunk_rows: int = 4096) -> None:
+        cb = batch.ctypes()
+        rc = lib().orc_agg_update(self.h, C.byref(cb), chunk_rows)
+        if rc:
+            raise OracleError(rc, lib().orc_last_error().decode())
+
+    def num_groups(self) -> int:
+        return lib().orc_agg_num_groups(self.h)
+
+    def emit(self, fp_mode: int = ORC_FP_COMPENSATED):
+        from vecruntime_b200.aggregate import _out_arrays
+
+        n = self.num_groups()
+        arrays = [_out_arrays(t, n) for t in self.output_types]
+        outs = (N.OutColumn * max(1, len(arrays)))()
+        for i, (d, v) in enumerate(arrays):
+            outs[i].data = d.ctypes.data
+            outs[i].validity = v.ctypes.data
+        rc = lib().orc_agg_emit(self.h, 0, n, outs, fp_mode)
+        if rc:
+            raise OracleError(rc, lib().orc_last_error().decode())
+        return arrays
+
+    def close(self):
+        if self.h:
+            lib().orc_agg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def hash_rows(columns, n: int, finish: bool = True) -> np.ndarray:
+    types = (N.ColumnType * max(1, len(columns)))(*[c.ctype() for c in columns])
+    cols = (N.Column * max(1, len(columns)))()
+    for i, c in enumerate(columns):
+        cols[i].data = c.data.ctypes.data
+        cols[i].validity = c.validity.ctypes.data if c.validity is not None else None
+    out = np.zeros(max(n, 1), np.uint32)
+    lib().orc_hash_rows(len(columns), types, cols, n, out.ctypes.data, 1 if finish else 0)
+    return out[:n]
+
+
+def run_threads(spec, batch, threads: int, chunk_rows: int = 4096):
+    """Times the oracle on `threads` host threads (one partition each, then
+    merged): returns (seconds, groups)."""
+    cb = batch.ctypes()
+    secs = C.c_double()
+    groups = C.c_int64()
+    rc = lib().orc_agg_run_threads(C.byref(spec.spec), C.byref(cb), threads, chunk_rows, C.byref(secs),
+                                   C.byref(groups))
+    if rc:
+        raise OracleError(rc, lib().orc_last_error().decode())
+    return secs.value, groups.value

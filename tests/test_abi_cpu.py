@@ -1,0 +1,114 @@
+"""CPU-only checks of the C ABI library: it loads, exports exactly what
+include/vrgpu.h declares, and its host-side planner (the GPU gate) compiles
+specs the way the reference's planner would accept or refuse them."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import vecruntime_b200 as vr
+from vecruntime_b200 import native as N
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    text = open(os.path.join(ROOT, "include", "vrgpu.h")).read()
+    return set(re.findall(r"^(?:int|void|const char\*|void\*)\s+(vr_[a-z0-9_]+)\(", text, re.M))
+
+
+def test_library_loads_and_exports_every_declared_symbol():
+    lib = N.lib()
+    declared = declared_symbols()
+    assert len(declared) > 30
+    for name in declared:
+        assert hasattr(lib, name), name
+    out = subprocess.run(["nm", "-D", "--defined-only", N.LIB_PATH], capture_output=True, text=True, check=True)
+    exported = {l.split()[-1] for l in out.stdout.splitlines() if " T " in l}
+    assert declared == exported, (declared ^ exported)
+
+
+def test_ctypes_prototypes_cover_the_header():
+    names = {p[0] for p in N.PROTOTYPES}
+    assert names == declared_symbols()
+
+
+def test_status_strings():
+    assert N.status_string(N.VR_OK) == "ok"
+    assert "overflow" in N.status_string(N.VR_ERR_OVERFLOW)
+
+
+def spec_of(cols, keys, fns, **kw):
+    return vr.Spec(cols, keys, fns, **kw)
+
+
+def test_plan_plain_int64_key_uses_sentinel_layout():
+    cols = [vr.longs(np.zeros(1, np.int64), nullable=False), vr.longs(np.zeros(1, np.int64), nullable=True),
+            vr.doubles(np.zeros(1), nullable=False)]
+    fns = [vr.CountAgg(), vr.CountAgg(1), vr.SumLongAgg(1, checked=True), vr.MinMaxAgg(1, True),
+           vr.MinMaxAgg(1, False), vr.SumDoubleAgg(2), vr.AverageAgg(2)]
+    rc, info, outs = spec_of(cols, [0], fns).plan()
+    assert rc == N.VR_OK
+    assert info.key_words == 1 and info.sentinel_layout == 1
+    assert info.direct_ok == 0
+    # keys + count, count, sum, min, max, sum, (avg sum, avg count)
+    assert [o.lane for o in outs] == [N.VR_INT64, N.VR_INT64, N.VR_INT64, N.VR_INT64, N.VR_INT64, N.VR_INT64,
+                                      N.VR_FLOAT64, N.VR_FLOAT64, N.VR_INT64]
+    # rows, count(v1), sum(v1), min(v1), max(v1), sum(v2); count(*) is the rows op and
+    # avg(v2)'s count of a non-nullable column is count(*) too: no extra ops
+    assert info.num_ops == 6
+
+
+def test_plan_dictionary_keys_are_direct_indexed():
+    cols = [vr.dict_ids(np.zeros(1), 3, nullable=False), vr.dict_ids(np.zeros(1), 2, nullable=True),
+            vr.decimals(np.zeros(1), 12, 2, nullable=False)]
+    fns = [vr.WideDecimalSumAgg(2, 22, 2), vr.CountAgg()]
+    rc, info, outs = spec_of(cols, [0, 1], fns).plan()
+    assert rc == N.VR_OK
+    assert info.direct_ok == 1 and info.direct_slots == 3 * 3  # (3) x (2 + null)
+    assert [o.lane for o in outs] == [N.VR_DICT32, N.VR_DICT32, N.VR_DECIMAL128, N.VR_BOOL, N.VR_INT64]
+    assert outs[2].precision == 22 and outs[2].scale == 2
+
+
+def test_plan_composite_nullable_key_needs_two_words():
+    cols = [vr.longs(np.zeros(1, np.int64), nullable=True), vr.ints(np.zeros(1), nullable=False),
+            vr.ints(np.zeros(1), nullable=False)]
+    rc, info, _ = spec_of(cols, [0, 1], [vr.CountAgg(), vr.SumLongAgg(2)]).plan()
+    assert rc == N.VR_OK and info.key_words == 2 and info.sentinel_layout == 0
+
+
+def test_plan_refuses_what_the_gpu_gate_does_not_cover():
+    cols = [vr.longs(np.zeros(1, np.int64), nullable=False), vr.decimals(np.zeros(1), 12, 2, nullable=False),
+            vr.decimals(np.zeros(1), 12, 3, nullable=False)]
+    # a decimal average's result needs Spark's division: stays on the CPU path
+    f = vr.AggFunction(N.VR_FN_AVG_DECIMAL, 1, flags=N.VR_FN_FINAL, precision=22, scale=2)
+    rc, info, _ = spec_of(cols, [0], [f]).plan()
+    assert rc == N.VR_ERR_UNSUPPORTED and b"division" in info.reason
+    # a product whose scale needs rounding
+    p = vr.DecimalProduct([(1, 1, 0), (2, 1, 0)])
+    rc, info, _ = spec_of(cols, [0], [vr.WideDecimalSumAgg(p, 38, 4)]).plan()
+    assert rc == N.VR_ERR_UNSUPPORTED
+    # min over a boolean lane
+    cols2 = [vr.longs(np.zeros(1, np.int64), nullable=False), vr.bools(np.zeros(1, bool))]
+    rc, info, _ = spec_of(cols2, [0], [vr.MinMaxAgg(1, True)]).plan()
+    assert rc == N.VR_ERR_UNSUPPORTED
+
+
+def test_plan_too_many_accumulators_is_refused():
+    cols = [vr.longs(np.zeros(1, np.int64), nullable=False)] + [vr.decimals128([0], 38, 0) for _ in range(15)]
+    fns = [vr.WideDecimalSumAgg(i, 38, 0) for i in range(1, 16)] * 3
+    rc, info, _ = spec_of(cols, [0], fns).plan()
+    assert rc == N.VR_ERR_UNSUPPORTED
+
+
+def test_create_without_gpu_fails_loudly():
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    cols = [vr.longs(np.zeros(1, np.int64), nullable=False)]
+    with pytest.raises(vr.VrError):
+        vr.GpuHashAggregate(cols, [0], [vr.CountAgg()])

@@ -1,0 +1,990 @@
+// C ABI of libvrgpu: handle lifecycle, staging, launches, growth, emission.
+//
+// The handle mirrors the reference's per-task aggregate state
+// (VectorGroupedAggregateIterator, VectorHashAggregateExec.scala:463-1039):
+// update = consume(batch) (:584-602), num_groups = table.size(), emit =
+// buildBatch(from, to) (:831-913), reset = EmitAndReset (:193-246), destroy =
+// close (:999-1019). One handle per task thread; each owns a CUDA stream.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+
+#include "runtime.h"
+#include "tune.h"
+
+namespace vr {
+
+static thread_local std::string t_last_error;
+void set_thread_error(const std::string& msg) { t_last_error = msg; }
+
+int set_err(vr_agg* h, int code, const std::string& msg) {
+    if (h) {
+        if (h->status == VR_OK) {
+            h->status = code;
+            h->last_error = msg;
+        }
+        if (code != VR_ERR_INVALID && code != VR_ERR_UNSUPPORTED) h->dead = true;
+    }
+    t_last_error = msg;
+    return code;
+}
+
+int cuda_err(vr_agg* h, cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return VR_OK;
+    std::string msg = std::string(what) + ": " + cudaGetErrorString(e);
+    if (e == cudaErrorMemoryAllocation) return set_err(h, VR_ERR_OOM, msg);
+    return set_err(h, VR_ERR_CUDA, msg);
+}
+
+static std::mutex g_dev_mu;
+static DeviceInfo g_dev[64];
+
+DeviceInfo& device_info(int device) {
+    std::lock_guard<std::mutex> lk(g_dev_mu);
+    DeviceInfo& d = g_dev[device & 63];
+    if (!d.ready) {
+        int prev = 0;
+        cudaGetDevice(&prev);
+        cudaSetDevice(device);
+        cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, device);
+        cudaDeviceGetAttribute(&d.smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+        upload_pow10();
+        cudaSetDevice(prev);
+        d.ready = true;
+    }
+    return d;
+}
+
+static int64_t next_pow2(int64_t x) {
+    int64_t p = 1;
+    while (p < x) p <<= 1;
+    return p;
+}
+static size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+static int32_t stage_bytes_for(const Program& P, int T) {
+    int32_t b = 0;
+    for (int c = 0; c < P.num_cols; ++c) {
+        int w = P.col_width[c];
+        b += (int32_t)al256(w ? (size_t)T * w : (size_t)T / 8);
+        if (P.col_nullable[c]) b += (int32_t)al256((size_t)T / 8);
+    }
+    b += (int32_t)al256((size_t)T / 8);  // selection
+    return b;
+}
+
+static void fill_layout(const Program& P, int T, StageLayout& L) {
+    int32_t off = 0;
+    for (int c = 0; c < kMaxCols; ++c) {
+        L.data_off[c] = -1;
+        L.valid_off[c] = -1;
+    }
+    for (int c = 0; c < P.num_cols; ++c) {
+        int w = P.col_width[c];
+        L.data_off[c] = off;
+        off += (int32_t)al256(w ? (size_t)T * w : (size_t)T / 8);
+        if (P.col_nullable[c]) {
+            L.valid_off[c] = off;
+            off += (int32_t)al256((size_t)T / 8);
+        }
+    }
+    L.sel_off = off;
+    off += (int32_t)al256((size_t)T / 8);
+    L.stage_bytes = off;
+}
+
+int64_t tiles_for(const vr_agg* h, int64_t rows) { return (rows + h->cfg.tile_rows - 1) / h->cfg.tile_rows; }
+
+// Picks tier, block shape, tile and shared-cache sizes. `forced` (tests /
+// tuner) overrides the defaults field by field.
+static int choose_config(vr_agg* h, const vr_tune_choice* forced) {
+    const Program& P = h->plan.prog;
+    const DeviceInfo& di = device_info(h->device);
+    const int budget = di.smem_optin;
+    const int fl = h->spec.flags;
+    Config c;
+    int64_t est = h->spec.est_groups > 0 ? h->spec.est_groups : 0;
+    int want_tier = -1;  // from force flags / choice
+    if (fl & VR_SPEC_FORCE_DIRECT) want_tier = 0;
+    if (fl & VR_SPEC_FORCE_SHARED) want_tier = 1;
+    if (fl & VR_SPEC_FORCE_GLOBAL) want_tier = 2;
+    if (forced) want_tier = forced->tier;
+    if (want_tier == 0 && !h->plan.direct_ok)
+        return set_err(h, VR_ERR_UNSUPPORTED, "direct tier needs dictionary or boolean keys");
+
+    auto fits = [&](int stages, int T, int tier_bytes) {
+        return smem_map(stages, stage_bytes_for(P, T), tier_bytes).total <= budget;
+    };
+    bool chosen = false;
+    if (h->plan.direct_ok && (want_tier == -1 || want_tier == 0)) {
+        const int nts[] = {256, 192, 128, 96, 64};
+        const int Ts[] = {2048, 1024, 512};
+        for (int nt : nts) {
+            if (forced && forced->threads && nt != forced->threads) continue;
+            int64_t tb = P.direct_slots * P.aw * (int64_t)nt * 8;
+            if (tb > budget) continue;
+            for (int T : Ts) {
+                if (forced && forced->tile_rows && T != forced->tile_rows) continue;
+                for (int st = 3; st >= 2 && !chosen; --st) {
+                    if (fits(st, T, (int)tb)) {
+                        c.tier = kTierDirect;
+                        c.threads = nt;
+                        c.tile_rows = T;
+                        c.stages = st;
+                        chosen = true;
+                    }
+                }
+                if (chosen) break;
+            }
+            if (chosen) break;
+        }
+        if (!chosen && want_tier == 0) return set_err(h, VR_ERR_UNSUPPORTED, "direct tier does not fit in shared memory");
+    }
+    if (!chosen) {
+        c.tier = kTierHash;
+        c.threads = forced && forced->threads ? forced->threads : 256;
+        c.tile_rows = forced && forced->tile_rows ? forced->tile_rows : 2048;
+        int64_t g = est > 0 ? est : std::min<int64_t>(h->spec.max_batch_rows > 0 ? h->spec.max_batch_rows : (1 << 20), 1 << 20);
+        c.capacity = forced && forced->table_capacity ? next_pow2(forced->table_capacity) : next_pow2(std::max<int64_t>(1024, 2 * g));
+        bool use_cache = want_tier != 2;
+        c.stages = 3;
+        while (c.stages > 2 && !fits(c.stages, c.tile_rows, 0)) --c.stages;
+        while (!fits(c.stages, c.tile_rows, 0) && c.tile_rows > 256) c.tile_rows /= 2;
+        int free_bytes = budget - smem_map(c.stages, stage_bytes_for(P, c.tile_rows), 0).total;
+        int max_slots = free_bytes > 0 ? free_bytes / (8 * P.sw) : 0;
+        int slots = 1;
+        while (slots * 2 <= max_slots) slots *= 2;
+        if (max_slots < 1) slots = 0;
+        if (use_cache && slots >= 64) {
+            int64_t need = next_pow2(std::max<int64_t>(64, 2 * (est > 0 ? est : 1 << 30)));
+            if (need <= slots) {
+                c.smem_slots = (int)need;  // every group fits: a private table per CTA
+            } else {
+                c.smem_slots = std::min(slots, 2048);  // hot-key cache in front of HBM
+            }
+            if (forced && forced->smem_slots) c.smem_slots = std::min<int>(slots, (int)next_pow2(forced->smem_slots));
+        } else {
+            c.smem_slots = 0;
+        }
+        c.warp_agg = (est > 0 && est <= 4096) ? 1 : 0;
+    }
+    if (fl & VR_SPEC_WARP_AGG) c.warp_agg = 1;
+    if (fl & VR_SPEC_NO_WARP_AGG) c.warp_agg = 0;
+    if (forced) c.warp_agg = forced->warp_agg;
+    if (fl & VR_SPEC_NO_TMA) c.tma = 0;
+    const int tier_bytes = c.tier == kTierDirect ? (int)(P.direct_slots * P.aw * (int64_t)c.threads * 8)
+                                                 : c.smem_slots * P.sw * 8;
+    SmemMap m = smem_map(c.stages, stage_bytes_for(P, c.tile_rows), tier_bytes);
+    c.blocks_per_sm = (2 * m.total <= budget) ? 2 : 1;
+    if (forced && forced->blocks_per_sm) c.blocks_per_sm = forced->blocks_per_sm;
+    if (m.total > budget) return set_err(h, VR_ERR_UNSUPPORTED, "configuration exceeds shared memory");
+    if (c.threads % 32 || c.threads > kMaxConsumerThreads || c.tile_rows % 128)
+        return set_err(h, VR_ERR_INVALID, "bad forced block shape");
+    h->cfg = c;
+    LaunchCfg& L = h->launch;
+    std::memset(&L, 0, sizeof(L));
+    L.tile_rows = c.tile_rows;
+    L.stages = c.stages;
+    L.consumer_threads = c.threads;
+    L.num_desc = 1;
+    L.g_probes = c.g_probes;
+    L.s_probes = c.s_probes;
+    fill_layout(P, c.tile_rows, L.lay);
+    L.tier_bytes = tier_bytes;
+    L.smem_bytes = m.total;
+    h->blocks = di.sms * c.blocks_per_sm;
+    return VR_OK;
+}
+
+static int alloc_table(vr_agg* h) {
+    const Program& P = h->plan.prog;
+    int64_t slots = h->cfg.tier == kTierDirect ? P.direct_slots : h->cfg.capacity + 1;  // +1: sentinel side slot
+    size_t bytes = (size_t)slots * P.sw * 8;
+    cudaError_t e = cudaMalloc(&h->table, bytes);
+    if (e != cudaSuccess) return cuda_err(h, e, "table allocation");
+    e = cudaMemsetAsync(h->table, 0, bytes, h->stream);
+    if (e != cudaSuccess) return cuda_err(h, e, "table clear");
+    h->table_slots = slots;
+    h->stats.table_capacity = h->cfg.tier == kTierDirect ? P.direct_slots : h->cfg.capacity;
+    return VR_OK;
+}
+
+static int alloc_slot(vr_agg* h, StageSlot& s) {
+    cudaError_t e;
+    if ((e = cudaMallocHost(&s.desc_host, sizeof(BatchDesc))) != cudaSuccess) return cuda_err(h, e, "pinned desc");
+    if ((e = cudaMalloc(&s.desc_dev, sizeof(BatchDesc))) != cudaSuccess) return cuda_err(h, e, "desc");
+    if ((e = cudaMalloc(&s.ctrl_dev, CTRL_WORDS * 8)) != cudaSuccess) return cuda_err(h, e, "ctrl");
+    if ((e = cudaMallocHost(&s.ctrl_host, CTRL_WORDS * 8)) != cudaSuccess) return cuda_err(h, e, "pinned ctrl");
+    std::memset(s.ctrl_host, 0, CTRL_WORDS * 8);
+    if ((e = cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming)) != cudaSuccess) return cuda_err(h, e, "event");
+    if ((e = cudaEventCreate(&s.t0)) != cudaSuccess) return cuda_err(h, e, "event");
+    if ((e = cudaEventCreate(&s.t1)) != cudaSuccess) return cuda_err(h, e, "event");
+    if ((e = cudaEventCreate(&s.h0)) != cudaSuccess) return cuda_err(h, e, "event");
+    if ((e = cudaEventCreateWithFlags(&s.copied, cudaEventDisableTiming)) != cudaSuccess) return cuda_err(h, e, "event");
+    if (h->cfg.tier != kTierDirect) {
+        // spill list: every shared slot of every CTA, the most one launch can spill
+        s.spill_cap = (int64_t)h->blocks * std::max(1, h->cfg.smem_slots);
+        if ((e = cudaMalloc(&s.spill, (size_t)s.spill_cap * h->plan.prog.sw * 8)) != cudaSuccess)
+            return cuda_err(h, e, "spill list");
+    }
+    return VR_OK;
+}
+
+static int ensure_deferred(vr_agg* h, StageSlot& s, int64_t rows) {
+    if (h->cfg.tier == kTierDirect || s.deferred_cap >= rows) return VR_OK;
+    cudaFree(s.deferred);
+    cudaFree(s.deferred_tmp);
+    s.deferred = s.deferred_tmp = nullptr;
+    int64_t cap = std::max<int64_t>(rows, 4096);
+    cudaError_t e = cudaMalloc(&s.deferred, (size_t)cap * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&s.deferred_tmp, (size_t)cap * 8);
+    if (e != cudaSuccess) return cuda_err(h, e, "deferred list");
+    s.deferred_cap = cap;
+    return VR_OK;
+}
+
+int agg_build(const vr_agg_spec* spec, const vr_tune_choice* forced, vr_agg** out, cudaStream_t stream) {
+    if (!spec || !out) {
+        set_thread_error("null argument");
+        return VR_ERR_INVALID;
+    }
+    *out = nullptr;
+    vr_agg* h = new (std::nothrow) vr_agg();
+    if (!h) return VR_ERR_OOM;
+    h->columns.assign(spec->columns, spec->columns + spec->num_columns);
+    h->keys.assign(spec->key_columns, spec->key_columns + spec->num_keys);
+    h->fns.assign(spec->fns, spec->fns + spec->num_fns);
+    h->spec = *spec;
+    h->spec.columns = h->columns.data();
+    h->spec.key_columns = h->keys.data();
+    h->spec.fns = h->fns.data();
+    h->device = spec->device;
+    h->trace = (spec->flags & VR_SPEC_TRACE) != 0;
+    int rc = compile_plan(h->spec, h->plan);
+    if (rc != VR_OK) {
+        set_thread_error(h->plan.reason);
+        delete h;
+        return rc;
+    }
+    cudaError_t e = cudaSetDevice(h->device);
+    if (e != cudaSuccess) {
+        set_thread_error(std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+        delete h;
+        return VR_ERR_CUDA;
+    }
+    vr_tune_choice tuned;
+    if (!forced && tune_lookup_internal(h->spec, h->spec.max_batch_rows, &tuned)) forced = &tuned;
+    rc = choose_config(h, forced);
+    if (rc != VR_OK) {
+        std::string why = h->last_error;
+        delete h;
+        set_thread_error(why);
+        return rc;
+    }
+    if (stream) {
+        h->stream = stream;
+    } else if ((e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess) {
+        set_thread_error(std::string("stream: ") + cudaGetErrorString(e));
+        delete h;
+        return VR_ERR_CUDA;
+    } else {
+        h->own_stream = true;
+    }
+    if ((e = cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking)) != cudaSuccess) {
+        set_thread_error(std::string("copy stream: ") + cudaGetErrorString(e));
+        if (h->own_stream) cudaStreamDestroy(h->stream);
+        delete h;
+        return VR_ERR_CUDA;
+    }
+    h->stats.tier = h->cfg.tier == kTierDirect ? 0 : (h->cfg.smem_slots > 0 ? 1 : 2);
+    h->stats.warp_agg = h->cfg.warp_agg;
+    h->stats.slot_bytes = h->plan.prog.sw * 8;
+    h->stats.threads = h->cfg.threads;
+    h->stats.blocks = h->blocks;
+    h->stats.smem_bytes = h->launch.smem_bytes;
+    h->stats.tile_rows = h->cfg.tile_rows;
+    if ((e = cudaMalloc(&h->prog_dev, sizeof(Program))) != cudaSuccess ||
+        (e = cudaMalloc(&h->emit_dev, sizeof(EmitProgram))) != cudaSuccess ||
+        (e = cudaMemcpy(h->prog_dev, &h->plan.prog, sizeof(Program), cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(h->emit_dev, &h->plan.emit, sizeof(EmitProgram), cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMalloc(&h->num_dev, 8)) != cudaSuccess ||
+        (e = cudaMalloc(&h->outs_dev, sizeof(vr_out_column) * kMaxOut)) != cudaSuccess ||
+        (e = cudaMallocHost(&h->outs_host, sizeof(vr_out_column) * kMaxOut)) != cudaSuccess ||
+        (e = cudaMallocHost(&h->emit_ctrl, 64)) != cudaSuccess ||
+        (e = cudaMallocHost(&h->aux_desc_host, sizeof(BatchDesc))) != cudaSuccess ||
+        (e = cudaMalloc(&h->aux_desc_dev, sizeof(BatchDesc))) != cudaSuccess ||
+        (e = cudaMalloc(&h->aux_ctrl_dev, CTRL_WORDS * 8)) != cudaSuccess ||
+        (e = cudaMallocHost(&h->aux_ctrl_host, CTRL_WORDS * 8)) != cudaSuccess) {
+        cuda_err(h, e, "handle allocation");
+        std::string why = h->last_error;
+        vr_agg_destroy(h);
+        set_thread_error(why);
+        return e == cudaErrorMemoryAllocation ? VR_ERR_OOM : VR_ERR_CUDA;
+    }
+    rc = alloc_table(h);
+    for (int i = 0; i < 2 && rc == VR_OK; ++i) rc = alloc_slot(h, h->slot[i]);
+    if (rc == VR_OK) {
+        e = cudaStreamSynchronize(h->stream);
+        if (e != cudaSuccess) rc = cuda_err(h, e, "create");
+    }
+    if (rc != VR_OK) {
+        std::string why = h->last_error;
+        vr_agg_destroy(h);
+        set_thread_error(why);
+        return rc;
+    }
+    *out = h;
+    return VR_OK;
+}
+
+// Batch -> staged column pointers (host batches are copied into slot memory).
+static int stage_batch(vr_agg* h, StageSlot& s, const vr_batch& b, const char** data, const uint32_t** valid,
+                       const uint32_t** sel) {
+    const Plan& plan = h->plan;
+    const Program& P = plan.prog;
+    const int64_t n = b.num_rows;
+    if (b.location == VR_DEVICE) {
+        for (int c = 0; c < P.num_cols; ++c) {
+            const vr_column& col = b.columns[plan.spec_of_staged[c]];
+            data[c] = (const char*)col.data;
+            valid[c] = (const uint32_t*)col.validity;
+            if (((uintptr_t)col.validity & 3) != 0)
+                return set_err(h, VR_ERR_INVALID, "validity bitmaps must be 4-byte aligned");
+            if (!data[c] && n > 0) return set_err(h, VR_ERR_INVALID, "null column data");
+        }
+        *sel = (const uint32_t*)b.selection;
+        if (((uintptr_t)b.selection & 3) != 0) return set_err(h, VR_ERR_INVALID, "selection must be 4-byte aligned");
+        s.staged_h2d = false;
+        return VR_OK;
+    }
+    // host batch: one H2D copy per buffer into the slot's staging area
+    size_t need = 0;
+    for (int c = 0; c < P.num_cols; ++c) {
+        int w = P.col_width[c];
+        need += al256(w ? (size_t)n * w : (size_t)(n + 7) / 8 + 4);
+        need += al256((size_t)(n + 7) / 8 + 4);
+    }
+    need += al256((size_t)(n + 7) / 8 + 4);
+    if (need > s.dev_cap) {
+        if (s.dev) {
+            cudaError_t e = cudaFree(s.dev);
+            if (e != cudaSuccess) return cuda_err(h, e, "staging free");
+        }
+        s.dev = nullptr;
+        size_t cap = std::max(need, s.dev_cap + s.dev_cap / 2);
+        cudaError_t e = cudaMalloc(&s.dev, cap);
+        if (e != cudaSuccess) {
+            s.dev_cap = 0;
+            return cuda_err(h, e, "staging allocation");
+        }
+        s.dev_cap = cap;
+    }
+    cudaStream_t cs = h->copy_stream;
+    // copies of this slot wait until the kernel that last read it is done
+    if (s.pending_done_recorded) cudaStreamWaitEvent(cs, s.done, 0);
+    if (h->trace) cudaEventRecord(s.h0, cs);
+    size_t off = 0;
+    int64_t bytes_in = 0;
+    for (int c = 0; c < P.num_cols; ++c) {
+        const vr_column& col = b.columns[plan.spec_of_staged[c]];
+        int w = P.col_width[c];
+        size_t db = w ? (size_t)n * w : (size_t)(n + 7) / 8;
+        char* dst = s.dev + off;
+        if (n > 0) {
+            if (!col.data) return set_err(h, VR_ERR_INVALID, "null column data");
+            cudaError_t e = cudaMemcpyAsync(dst, col.data, db, cudaMemcpyHostToDevice, cs);
+            if (e != cudaSuccess) return cuda_err(h, e, "H2D");
+            bytes_in += (int64_t)db;
+        }
+        data[c] = dst;
+        off += al256(w ? (size_t)n * w : (size_t)(n + 7) / 8 + 4);
+        if (col.validity && n > 0) {
+            size_t vb = (size_t)(n + 7) / 8;
+            cudaError_t e = cudaMemcpyAsync(s.dev + off, col.validity, vb, cudaMemcpyHostToDevice, cs);
+            if (e != cudaSuccess) return cuda_err(h, e, "H2D");
+            valid[c] = (const uint32_t*)(s.dev + off);
+            bytes_in += (int64_t)vb;
+        } else {
+            valid[c] = nullptr;
+        }
+        off += al256((size_t)(n + 7) / 8 + 4);
+    }
+    if (b.selection && n > 0) {
+        size_t vb = (size_t)(n + 7) / 8;
+        cudaError_t e = cudaMemcpyAsync(s.dev + off, b.selection, vb, cudaMemcpyHostToDevice, cs);
+        if (e != cudaSuccess) return cuda_err(h, e, "H2D");
+        *sel = (const uint32_t*)(s.dev + off);
+        bytes_in += (int64_t)vb;
+    } else {
+        *sel = nullptr;
+    }
+    // the kernel (on the compute stream) starts once this slot's copies landed;
+    // the other slot's copies may meanwhile overlap the previous kernel
+    cudaError_t e = cudaEventRecord(s.copied, cs);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(h->stream, s.copied, 0);
+    if (e != cudaSuccess) return cuda_err(h, e, "copy ordering");
+    s.staged_h2d = true;
+    return VR_OK;
+}
+
+void fill_desc(vr_agg* h, const vr_batch& b, BatchDesc& d, uint64_t* ctrl, const StageSlot& s, int64_t tile_begin) {
+    (void)b;
+    d.num_rows = b.num_rows;
+    d.tile_begin = tile_begin;
+    d.num_tiles = tiles_for(h, b.num_rows);
+    d.table = h->table;
+    d.cap_mask = h->cfg.tier == kTierDirect ? h->plan.prog.direct_slots : h->cfg.capacity - 1;
+    d.ctrl = ctrl;
+    d.deferred = s.deferred;
+    d.deferred_cap = s.deferred_cap;
+    d.spill = s.spill;
+    d.spill_cap = s.spill_cap;
+    d.prog = h->prog_dev;
+    d.tier = h->cfg.tier;
+    d.smem_slots = h->cfg.smem_slots;
+    d.warp_agg = h->cfg.warp_agg;
+}
+
+static bool tma_ok(const vr_agg* h, const BatchDesc& d) {
+    if (!h->cfg.tma) return false;
+    for (int c = 0; c < h->plan.prog.num_cols; ++c) {
+        if (((uintptr_t)d.col_data[c] & 15) != 0) return false;
+        if (d.col_valid[c] && ((uintptr_t)d.col_valid[c] & 15) != 0) return false;
+    }
+    if (d.selection && ((uintptr_t)d.selection & 15) != 0) return false;
+    return true;
+}
+
+// Grows the HBM table to at least `need_groups` at load <= 1/2 and moves every
+// group over (k_merge_slots). Stream-ordered; the caller synchronises.
+static int grow_table(vr_agg* h, int64_t need_groups) {
+    const Program& P = h->plan.prog;
+    int64_t new_cap = std::max<int64_t>(2 * h->cfg.capacity, next_pow2(2 * need_groups));
+    uint64_t* old = h->table;
+    int64_t old_slots = h->table_slots;
+    size_t bytes = (size_t)(new_cap + 1) * P.sw * 8;
+    uint64_t* nt = nullptr;
+    cudaError_t e = cudaMalloc(&nt, bytes);
+    if (e != cudaSuccess) return cuda_err(h, e, "table grow");
+    if ((e = cudaMemsetAsync(nt, 0, bytes, h->stream)) != cudaSuccess) return cuda_err(h, e, "table grow");
+    h->table = nt;
+    h->cfg.capacity = new_cap;
+    h->table_slots = new_cap + 1;
+    BatchDesc d;
+    std::memset(&d, 0, sizeof(d));
+    vr_batch dummy{};
+    fill_desc(h, dummy, d, h->aux_ctrl_dev, h->slot[0], 0);
+    *h->aux_desc_host = d;
+    if ((e = cudaMemcpyAsync(h->aux_desc_dev, h->aux_desc_host, sizeof(BatchDesc), cudaMemcpyHostToDevice, h->stream)) !=
+        cudaSuccess)
+        return cuda_err(h, e, "desc");
+    if ((e = cudaMemsetAsync(h->aux_ctrl_dev, 0, CTRL_WORDS * 8, h->stream)) != cudaSuccess) return cuda_err(h, e, "ctrl");
+    if ((e = launch_merge_slots(P.kw, h->aux_desc_dev, old, old_slots, (int)std::min<int64_t>(new_cap, 1 << 20),
+                                h->stream)) != cudaSuccess)
+        return cuda_err(h, e, "rehash");
+    h->stats.kernel_launches++;
+    if ((e = cudaMemcpyAsync(h->aux_ctrl_host, h->aux_ctrl_dev, CTRL_WORDS * 8, cudaMemcpyDeviceToHost, h->stream)) !=
+        cudaSuccess)
+        return cuda_err(h, e, "ctrl");
+    if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) return cuda_err(h, e, "rehash");
+    if (h->aux_ctrl_host[CTRL_ERROR]) return set_err(h, VR_ERR_OOM, "rehash could not place every group");
+    cudaFree(old);
+    h->groups_known = (int64_t)h->aux_ctrl_host[CTRL_GROUPS];
+    h->stats.table_capacity = new_cap;
+    h->stats.rehashes++;
+    return VR_OK;
+}
+
+static int map_ctrl_error(vr_agg* h, uint64_t bits) {
+    if (bits & kErrBadKey) return set_err(h, VR_ERR_INVALID, "dictionary id outside its declared dictionary size");
+    if (bits & (kErrTimeout | kErrLockTimeout)) return set_err(h, VR_ERR_TIMEOUT, "a bounded device wait gave up");
+    if (bits & (kErrDeferredFull | kErrSpillFull)) return set_err(h, VR_ERR_OOM, "deferred/spill list overflow");
+    return set_err(h, VR_ERR_CUDA, "device error");
+}
+
+// Resolves every launched batch: errors, group counts, and rows or slots the
+// HBM table could not take (grow, merge spills, replay deferred rows).
+int agg_resolve_all(vr_agg* h) {
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return cuda_err(h, e, "update");
+    const Program& P = h->plan.prog;
+    int order[2] = {h->next_slot, h->next_slot ^ 1};  // oldest first
+    for (int k = 0; k < 2; ++k) {
+        StageSlot& s = h->slot[order[k]];
+        if (!s.pending) continue;
+        s.pending = false;
+        if (s.ctrl_host[CTRL_ERROR]) return map_ctrl_error(h, s.ctrl_host[CTRL_ERROR]);
+        h->groups_known += (int64_t)s.ctrl_host[CTRL_GROUPS];
+        if (s.timed) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, s.t0, s.t1);
+            h->stats.last_kernel_ms = ms;
+            h->stats.total_kernel_ms += ms;
+            if (s.staged_h2d) {
+                float hm = 0;
+                cudaEventElapsedTime(&hm, s.h0, s.t0);
+                h->stats.total_h2d_ms += hm;
+            }
+            s.timed = false;
+        }
+        int64_t deferred = (int64_t)s.ctrl_host[CTRL_DEFERRED];
+        int64_t spilled = (int64_t)s.ctrl_host[CTRL_SPILLED];
+        int guard = 0;
+        while ((deferred > 0 || spilled > 0) && guard++ < 8) {
+            int rc = grow_table(h, h->groups_known + deferred + spilled);
+            if (rc != VR_OK) return rc;
+            // the slot's batch descriptor, repointed at the grown table
+            BatchDesc d = s.launched;
+            d.table = h->table;
+            d.cap_mask = h->cfg.capacity - 1;
+            *s.desc_host = d;
+            if ((e = cudaMemcpyAsync(s.desc_dev, s.desc_host, sizeof(BatchDesc), cudaMemcpyHostToDevice, h->stream)) !=
+                cudaSuccess)
+                return cuda_err(h, e, "desc");
+            if (spilled > 0) {
+                if ((e = cudaMemsetAsync(s.ctrl_dev, 0, CTRL_WORDS * 8, h->stream)) != cudaSuccess)
+                    return cuda_err(h, e, "ctrl");
+                if ((e = launch_merge_slots(P.kw, s.desc_dev, s.spill, std::min(spilled, s.spill_cap), h->cfg.g_probes,
+                                            h->stream)) != cudaSuccess)
+                    return cuda_err(h, e, "spill merge");
+                h->stats.kernel_launches++;
+                if ((e = cudaMemcpyAsync(s.ctrl_host, s.ctrl_dev, CTRL_WORDS * 8, cudaMemcpyDeviceToHost, h->stream)) !=
+                    cudaSuccess)
+                    return cuda_err(h, e, "ctrl");
+                if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) return cuda_err(h, e, "spill merge");
+                if (s.ctrl_host[CTRL_ERROR]) return map_ctrl_error(h, s.ctrl_host[CTRL_ERROR]);
+                h->groups_known += (int64_t)s.ctrl_host[CTRL_GROUPS];
+                spilled = 0;
+            }
+            if (deferred > 0) {
+                int64_t n = std::min(deferred, s.deferred_cap);
+                h->stats.deferred_rows += n;
+                if ((e = cudaMemcpyAsync(s.deferred_tmp, s.deferred, (size_t)n * 8, cudaMemcpyDeviceToDevice,
+                                         h->stream)) != cudaSuccess)
+                    return cuda_err(h, e, "deferred copy");
+                if ((e = cudaMemsetAsync(s.ctrl_dev, 0, CTRL_WORDS * 8, h->stream)) != cudaSuccess)
+                    return cuda_err(h, e, "ctrl");
+                if ((e = launch_replay(P.kw, s.desc_dev, s.deferred_tmp, n, h->cfg.g_probes, h->stream)) != cudaSuccess)
+                    return cuda_err(h, e, "replay");
+                h->stats.kernel_launches++;
+                if ((e = cudaMemcpyAsync(s.ctrl_host, s.ctrl_dev, CTRL_WORDS * 8, cudaMemcpyDeviceToHost, h->stream)) !=
+                    cudaSuccess)
+                    return cuda_err(h, e, "ctrl");
+                if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) return cuda_err(h, e, "replay");
+                if (s.ctrl_host[CTRL_ERROR]) return map_ctrl_error(h, s.ctrl_host[CTRL_ERROR]);
+                h->groups_known += (int64_t)s.ctrl_host[CTRL_GROUPS];
+                deferred = (int64_t)s.ctrl_host[CTRL_DEFERRED];
+            }
+        }
+        if (deferred > 0 || spilled > 0) return set_err(h, VR_ERR_OOM, "table growth did not converge");
+    }
+    return VR_OK;
+}
+
+static int agg_update(vr_agg* h, const vr_batch* b) {
+    if (h->dead) return VR_ERR_STATE;
+    if (!b || b->num_rows < 0 || (b->num_rows > 0 && !b->columns))
+        return set_err(h, VR_ERR_INVALID, "bad batch");
+    if (b->num_rows == 0) return VR_OK;
+    cudaError_t e = cudaSetDevice(h->device);
+    if (e != cudaSuccess) return cuda_err(h, e, "cudaSetDevice");
+    StageSlot& s = h->slot[h->next_slot];
+    if (s.pending) {  // the batch that used this staging set two updates ago
+        if ((e = cudaEventSynchronize(s.done)) != cudaSuccess) return cuda_err(h, e, "update");
+        bool needs = s.ctrl_host[CTRL_ERROR] || s.ctrl_host[CTRL_DEFERRED] || s.ctrl_host[CTRL_SPILLED];
+        if (needs) {
+            int rc = agg_resolve_all(h);
+            if (rc != VR_OK) return rc;
+        } else {
+            s.pending = false;
+            h->groups_known += (int64_t)s.ctrl_host[CTRL_GROUPS];
+            if (s.timed) {
+                float ms = 0;
+                cudaEventElapsedTime(&ms, s.t0, s.t1);
+                h->stats.last_kernel_ms = ms;
+                h->stats.total_kernel_ms += ms;
+                if (s.staged_h2d) {
+                    float hm = 0;
+                    cudaEventElapsedTime(&hm, s.h0, s.t0);
+                    h->stats.total_h2d_ms += hm;
+                }
+                s.timed = false;
+            }
+        }
+    }
+    // keep the HBM table at load <= 1/2 of what is already known
+    if (h->cfg.tier != kTierDirect && h->groups_known * 2 > h->cfg.capacity) {
+        int rc = agg_resolve_all(h);
+        if (rc == VR_OK) rc = grow_table(h, h->groups_known);
+        if (rc != VR_OK) return rc;
+    }
+    int rc = ensure_deferred(h, s, b->num_rows);
+    if (rc != VR_OK) return rc;
+    BatchDesc d;
+    std::memset(&d, 0, sizeof(d));
+    const char* data[kMaxCols] = {};
+    const uint32_t* valid[kMaxCols] = {};
+    const uint32_t* sel = nullptr;
+    rc = stage_batch(h, s, *b, data, valid, &sel);
+    if (rc != VR_OK) return rc;
+    for (int c = 0; c < kMaxCols; ++c) {
+        d.col_data[c] = data[c];
+        d.col_valid[c] = valid[c];
+    }
+    d.selection = sel;
+    fill_desc(h, *b, d, s.ctrl_dev, s, 0);
+    d.tma = tma_ok(h, d) ? 1 : 0;
+    *s.desc_host = d;
+    s.launched = d;
+    if ((e = cudaMemcpyAsync(s.desc_dev, s.desc_host, sizeof(BatchDesc), cudaMemcpyHostToDevice, h->stream)) != cudaSuccess)
+        return cuda_err(h, e, "desc");
+    if ((e = cudaMemsetAsync(s.ctrl_dev, 0, CTRL_WORDS * 8, h->stream)) != cudaSuccess) return cuda_err(h, e, "ctrl");
+    LaunchCfg L = h->launch;
+    L.total_tiles = d.num_tiles;
+    int blocks = (int)std::min<int64_t>(h->blocks, d.num_tiles);
+    if (h->trace) cudaEventRecord(s.t0, h->stream);
+    if ((e = launch_aggregate(h->plan.prog.kw, h->cfg.tier, s.desc_dev, L, blocks, &s.ctrl_dev[CTRL_NEXT_TILE],
+                              h->stream)) != cudaSuccess)
+        return cuda_err(h, e, "aggregate launch");
+    if (h->trace) {
+        cudaEventRecord(s.t1, h->stream);
+        s.timed = true;
+    }
+    h->stats.kernel_launches++;
+    if ((e = cudaMemcpyAsync(s.ctrl_host, s.ctrl_dev, CTRL_WORDS * 8, cudaMemcpyDeviceToHost, h->stream)) != cudaSuccess)
+        return cuda_err(h, e, "ctrl");
+    if ((e = cudaEventRecord(s.done, h->stream)) != cudaSuccess) return cuda_err(h, e, "event");
+    s.pending_done_recorded = true;
+    s.pending = true;
+    s.rows = b->num_rows;
+    h->next_slot ^= 1;
+    h->compact_valid = false;
+    h->stats.rows += b->num_rows;
+    h->stats.batches++;
+    return VR_OK;
+}
+
+static int agg_compact(vr_agg* h) {
+    int rc = agg_resolve_all(h);
+    if (rc != VR_OK) return rc;
+    if (h->compact_valid) return VR_OK;
+    const Program& P = h->plan.prog;
+    cudaError_t e;
+    if (h->slot_of_cap < h->table_slots) {
+        cudaFree(h->slot_of);
+        h->slot_of = nullptr;
+        if ((e = cudaMalloc(&h->slot_of, (size_t)h->table_slots * 8)) != cudaSuccess) return cuda_err(h, e, "compaction");
+        h->slot_of_cap = h->table_slots;
+    }
+    size_t need = 0;
+    if ((e = launch_compact_kw(P.kw, h->table, h->table_slots, P.sw, h->slot_of, h->num_dev, nullptr, &need, h->stream)) !=
+        cudaSuccess)
+        return cuda_err(h, e, "compaction sizing");
+    if (need > h->cub_temp_bytes) {
+        cudaFree(h->cub_temp);
+        h->cub_temp = nullptr;
+        if ((e = cudaMalloc(&h->cub_temp, need)) != cudaSuccess) return cuda_err(h, e, "compaction scratch");
+        h->cub_temp_bytes = need;
+    }
+    size_t tb = h->cub_temp_bytes;
+    if ((e = launch_compact_kw(P.kw, h->table, h->table_slots, P.sw, h->slot_of, h->num_dev, h->cub_temp, &tb,
+                               h->stream)) != cudaSuccess)
+        return cuda_err(h, e, "compaction");
+    h->stats.kernel_launches += 2;
+    int64_t n = 0;
+    if ((e = cudaMemcpyAsync(h->emit_ctrl, h->num_dev, 8, cudaMemcpyDeviceToHost, h->stream)) != cudaSuccess)
+        return cuda_err(h, e, "compaction");
+    if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) return cuda_err(h, e, "compaction");
+    n = (int64_t)h->emit_ctrl[0];
+    h->num_groups = n;
+    h->stats.groups = n;
+    h->compact_valid = true;
+    return VR_OK;
+}
+
+static size_t out_data_bytes(int lane, int64_t n) {
+    switch (lane) {
+        case VR_INT32:
+        case VR_DICT32: return (size_t)n * 4;
+        case VR_INT64:
+        case VR_FLOAT64: return (size_t)n * 8;
+        case VR_DECIMAL128: return (size_t)n * 16;
+        case VR_BOOL: return (size_t)(n + 7) / 8;
+    }
+    return 0;
+}
+
+static int agg_emit(vr_agg* h, int64_t from, int64_t to, const vr_out_column* outs, int32_t location) {
+    if (h->dead) return VR_ERR_STATE;
+    int rc = agg_compact(h);
+    if (rc != VR_OK) return rc;
+    if (from < 0 || to < from || to > h->num_groups) return set_err(h, VR_ERR_INVALID, "emit range outside [0, groups]");
+    if (!outs) return set_err(h, VR_ERR_INVALID, "null output columns");
+    const int64_t n = to - from;
+    if (n == 0) return VR_OK;
+    const EmitProgram& E = h->plan.emit;
+    cudaError_t e;
+    if (location == VR_DEVICE) {
+        for (int j = 0; j < E.num_out; ++j) h->outs_host[j] = outs[j];
+    } else {
+        size_t need = 0;
+        for (int j = 0; j < E.num_out; ++j)
+            need += al256(out_data_bytes(E.outs[j].lane, n)) + al256((size_t)(n + 7) / 8);
+        if (need > h->emit_stage_cap) {
+            cudaFree(h->emit_stage);
+            h->emit_stage = nullptr;
+            if ((e = cudaMalloc(&h->emit_stage, need)) != cudaSuccess) return cuda_err(h, e, "emit staging");
+            h->emit_stage_cap = need;
+        }
+        size_t off = 0;
+        for (int j = 0; j < E.num_out; ++j) {
+            h->outs_host[j].data = h->emit_stage + off;
+            off += al256(out_data_bytes(E.outs[j].lane, n));
+            h->outs_host[j].validity = (uint8_t*)(h->emit_stage + off);
+            off += al256((size_t)(n + 7) / 8);
+        }
+    }
+    if ((e = cudaMemcpyAsync(h->outs_dev, h->outs_host, sizeof(vr_out_column) * E.num_out, cudaMemcpyHostToDevice,
+                             h->stream)) != cudaSuccess)
+        return cuda_err(h, e, "emit");
+    if ((e = cudaMemsetAsync(h->aux_ctrl_dev, 0, CTRL_WORDS * 8, h->stream)) != cudaSuccess) return cuda_err(h, e, "ctrl");
+    if ((e = launch_emit(h->prog_dev, h->emit_dev, h->table, h->slot_of, from, to, h->outs_dev, h->aux_ctrl_dev,
+                         h->stream)) !=
+        cudaSuccess)
+        return cuda_err(h, e, "emit launch");
+    h->stats.kernel_launches++;
+    if (location != VR_DEVICE) {
+        for (int j = 0; j < E.num_out; ++j) {
+            if (outs[j].data) {
+                e = cudaMemcpyAsync(outs[j].data, h->outs_host[j].data, out_data_bytes(E.outs[j].lane, n),
+                                    cudaMemcpyDeviceToHost, h->stream);
+                if (e != cudaSuccess) return cuda_err(h, e, "D2H");
+            }
+            if (outs[j].validity) {
+                e = cudaMemcpyAsync(outs[j].validity, h->outs_host[j].validity, (size_t)(n + 7) / 8,
+                                    cudaMemcpyDeviceToHost, h->stream);
+                if (e != cudaSuccess) return cuda_err(h, e, "D2H");
+            }
+        }
+    }
+    if ((e = cudaMemcpyAsync(h->aux_ctrl_host, h->aux_ctrl_dev, CTRL_WORDS * 8, cudaMemcpyDeviceToHost, h->stream)) !=
+        cudaSuccess)
+        return cuda_err(h, e, "ctrl");
+    if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) return cuda_err(h, e, "emit");
+    int st = (int)h->aux_ctrl_host[CTRL_EMIT_ERROR];
+    if (st != 0) {
+        const char* why = st == VR_ERR_OVERFLOW ? "long overflow (ANSI sum)"
+                          : st == VR_ERR_DECIMAL_OVERFLOW ? "overflow in sum of decimals (ANSI)"
+                                                          : "decimal result past its precision (ANSI)";
+        return set_err(h, st, why);
+    }
+    return VR_OK;
+}
+
+}  // namespace vr
+
+using namespace vr;
+
+extern "C" {
+
+int vr_agg_create(const vr_agg_spec* spec, vr_agg** out) { return agg_build(spec, nullptr, out, nullptr); }
+
+int vr_agg_create_tuned(const vr_agg_spec* spec, const vr_tune_choice* choice, vr_agg** out) {
+    return agg_build(spec, choice, out, nullptr);
+}
+
+int vr_agg_update(vr_agg* h, const vr_batch* b) {
+    if (!h) return VR_ERR_INVALID;
+    return agg_update(h, b);
+}
+
+int vr_agg_sync(vr_agg* h) {
+    if (!h) return VR_ERR_INVALID;
+    if (h->dead) return VR_ERR_STATE;
+    cudaSetDevice(h->device);
+    return agg_resolve_all(h);
+}
+
+int vr_agg_num_groups(vr_agg* h, int64_t* groups) {
+    if (!h || !groups) return VR_ERR_INVALID;
+    if (h->dead) return VR_ERR_STATE;
+    cudaSetDevice(h->device);
+    int rc = agg_compact(h);
+    if (rc == VR_OK) *groups = h->num_groups;
+    return rc;
+}
+
+int vr_agg_output_schema(const vr_agg* h, int32_t* num_out, vr_column_type* types, int32_t cap) {
+    if (!h || !num_out) return VR_ERR_INVALID;
+    *num_out = (int32_t)h->plan.out_types.size();
+    if (types)
+        for (int32_t i = 0; i < *num_out && i < cap; ++i) types[i] = h->plan.out_types[i];
+    return VR_OK;
+}
+
+int vr_agg_emit(vr_agg* h, int64_t from, int64_t to, const vr_out_column* outs, int32_t location) {
+    if (!h) return VR_ERR_INVALID;
+    cudaSetDevice(h->device);
+    return agg_emit(h, from, to, outs, location);
+}
+
+int vr_agg_reset(vr_agg* h) {
+    if (!h) return VR_ERR_INVALID;
+    if (h->dead) return VR_ERR_STATE;
+    cudaSetDevice(h->device);
+    int rc = agg_resolve_all(h);
+    if (rc != VR_OK) return rc;
+    cudaError_t e = cudaMemsetAsync(h->table, 0, (size_t)h->table_slots * h->plan.prog.sw * 8, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return cuda_err(h, e, "reset");
+    h->groups_known = 0;
+    h->compact_valid = false;
+    h->num_groups = 0;
+    return VR_OK;
+}
+
+void vr_agg_destroy(vr_agg* h) {
+    if (!h) return;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (auto& s : h->slot) {
+        cudaFree(s.dev);
+        cudaFreeHost(s.desc_host);
+        cudaFree(s.desc_dev);
+        cudaFree(s.ctrl_dev);
+        cudaFreeHost(s.ctrl_host);
+        cudaFree(s.deferred);
+        cudaFree(s.deferred_tmp);
+        cudaFree(s.spill);
+        if (s.done) cudaEventDestroy(s.done);
+        if (s.t0) cudaEventDestroy(s.t0);
+        if (s.t1) cudaEventDestroy(s.t1);
+        if (s.h0) cudaEventDestroy(s.h0);
+        if (s.copied) cudaEventDestroy(s.copied);
+    }
+    cudaFree(h->table);
+    cudaFree(h->prog_dev);
+    cudaFree(h->emit_dev);
+    cudaFree(h->slot_of);
+    cudaFree(h->num_dev);
+    cudaFree(h->cub_temp);
+    cudaFree(h->outs_dev);
+    cudaFreeHost(h->outs_host);
+    cudaFree(h->emit_stage);
+    cudaFreeHost(h->emit_ctrl);
+    cudaFreeHost(h->aux_desc_host);
+    cudaFree(h->aux_desc_dev);
+    cudaFree(h->aux_ctrl_dev);
+    cudaFreeHost(h->aux_ctrl_host);
+    if (h->copy_stream) {
+        cudaStreamSynchronize(h->copy_stream);
+        cudaStreamDestroy(h->copy_stream);
+    }
+    if (h->stream && h->own_stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+int vr_agg_get_stats(const vr_agg* h, vr_agg_stats* st) {
+    if (!h || !st) return VR_ERR_INVALID;
+    *st = h->stats;
+    st->groups = h->compact_valid ? h->num_groups : h->groups_known;
+    return VR_OK;
+}
+
+int vr_agg_last_error(const vr_agg* h, char* buf, size_t cap) {
+    if (!h || !buf || cap == 0) return VR_ERR_INVALID;
+    std::snprintf(buf, cap, "%s", h->last_error.c_str());
+    return VR_OK;
+}
+
+const char* vr_thread_last_error(void) { return t_last_error.c_str(); }
+
+const char* vr_status_string(int s) {
+    switch (s) {
+        case VR_OK: return "ok";
+        case VR_ERR_INVALID: return "invalid argument";
+        case VR_ERR_OOM: return "out of memory";
+        case VR_ERR_OVERFLOW: return "arithmetic overflow";
+        case VR_ERR_DECIMAL_PRECISION: return "decimal precision exceeded";
+        case VR_ERR_TIMEOUT: return "device wait timed out";
+        case VR_ERR_CUDA: return "CUDA error";
+        case VR_ERR_UNSUPPORTED: return "unsupported on the GPU";
+        case VR_ERR_STATE: return "handle is dead or call out of order";
+        case VR_ERR_ADMISSION: return "request exceeds the admission cap";
+        case VR_ERR_DECIMAL_OVERFLOW: return "overflow in sum of decimals";
+    }
+    return "unknown status";
+}
+
+void* vr_agg_stream(const vr_agg* h) { return h ? (void*)h->stream : nullptr; }
+
+int vr_host_alloc(size_t bytes, void** out) {
+    if (!out) return VR_ERR_INVALID;
+    cudaError_t e = cudaHostAlloc(out, bytes, cudaHostAllocPortable);
+    if (e != cudaSuccess) {
+        t_last_error = cudaGetErrorString(e);
+        return VR_ERR_OOM;
+    }
+    return VR_OK;
+}
+int vr_host_free(void* p) { return cudaFreeHost(p) == cudaSuccess ? VR_OK : VR_ERR_CUDA; }
+int vr_host_register(void* p, size_t bytes) {
+    cudaError_t e = cudaHostRegister(p, bytes, cudaHostRegisterPortable);
+    if (e != cudaSuccess) {
+        t_last_error = cudaGetErrorString(e);
+        return VR_ERR_CUDA;
+    }
+    return VR_OK;
+}
+int vr_host_unregister(void* p) { return cudaHostUnregister(p) == cudaSuccess ? VR_OK : VR_ERR_CUDA; }
+
+int vr_hash_rows(int32_t num_keys, const vr_column_type* types, const vr_column* keys, int64_t num_rows,
+                 uint32_t* out_device, int32_t finish, void* stream) {
+    if (num_keys < 0 || num_keys > 16 || (num_keys > 0 && (!types || !keys)) || !out_device) return VR_ERR_INVALID;
+    cudaStream_t st = (cudaStream_t)stream;
+    vr_column_type* td = nullptr;
+    vr_column* kd = nullptr;
+    cudaError_t e = cudaMalloc(&td, sizeof(vr_column_type) * 16);
+    if (e == cudaSuccess) e = cudaMalloc(&kd, sizeof(vr_column) * 16);
+    if (e == cudaSuccess && num_keys > 0)
+        e = cudaMemcpyAsync(td, types, sizeof(vr_column_type) * num_keys, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && num_keys > 0) e = cudaMemcpyAsync(kd, keys, sizeof(vr_column) * num_keys, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = launch_hash_rows(num_keys, td, kd, num_rows, out_device, finish, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(td);
+    cudaFree(kd);
+    if (e != cudaSuccess) {
+        t_last_error = cudaGetErrorString(e);
+        return VR_ERR_CUDA;
+    }
+    return VR_OK;
+}
+
+int vr_agg_plan(const vr_agg_spec* spec, vr_plan_info* info, vr_column_type* out_types, int32_t cap) {
+    if (!spec || !info) return VR_ERR_INVALID;
+    std::memset(info, 0, sizeof(*info));
+    Plan plan;
+    int rc = compile_plan(*spec, plan);
+    std::snprintf(info->reason, sizeof(info->reason), "%s", plan.reason.c_str());
+    if (rc != VR_OK) return rc;
+    const Program& P = plan.prog;
+    info->key_words = P.kw;
+    info->acc_words = P.aw;
+    info->slot_words = P.sw;
+    info->num_ops = P.num_ops;
+    info->num_outputs = plan.emit.num_out;
+    info->staged_columns = P.num_cols;
+    info->sentinel_layout = P.occ_word < 0 ? 1 : 0;
+    info->direct_ok = plan.direct_ok ? 1 : 0;
+    info->direct_slots = P.direct_slots;
+    if (out_types)
+        for (int i = 0; i < plan.emit.num_out && i < cap; ++i) out_types[i] = plan.out_types[i];
+    return VR_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,281 @@
+// Batched aggregation: many independent instances (Spark tasks' batches of
+// uneven row counts and cardinalities) in ONE persistent launch of
+// k_aggregate. Tiles of every instance form one work space; CTAs pull tiles
+// from a global counter, so a CTA that finishes a small instance moves on to
+// the next tile of any instance. The whole step (table clears + the
+// persistent launch) can be captured once as a CUDA graph and replayed.
+//
+// VR_BATCHED_PLAIN runs the same instances with one clear + one launch per
+// instance, the baseline the persistent form is measured against.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "runtime.h"
+
+namespace vr {
+
+struct ZeroSpan {
+    uint64_t* ptr;
+    int64_t words;
+};
+
+// Zeroes many buffers in one launch: block b takes span b % n with a stride.
+__global__ void k_zero_many(const ZeroSpan* __restrict__ spans, int n) {
+    for (int s = blockIdx.y; s < n; s += gridDim.y) {
+        uint64_t* p = spans[s].ptr;
+        const int64_t w = spans[s].words;
+        for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < w; i += (int64_t)gridDim.x * blockDim.x)
+            p[i] = 0;
+    }
+}
+
+// Gathers every instance's control block into one array (one D2H copy).
+__global__ void k_gather_ctrl(const BatchDesc* __restrict__ descs, int n, uint64_t* __restrict__ out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n * CTRL_WORDS; i += gridDim.x * blockDim.x)
+        out[i] = descs[i / CTRL_WORDS].ctrl[i % CTRL_WORDS];
+}
+
+}  // namespace vr
+
+struct vr_batched {
+    int device = 0;
+    int mode = VR_BATCHED_PERSISTENT;
+    bool use_graph = false;
+    std::vector<vr_agg*> inst;
+    std::vector<vr::BatchDesc> descs;
+    vr::BatchDesc* descs_dev = nullptr;
+    vr::ZeroSpan* spans_dev = nullptr;
+    int num_spans = 0;
+    uint64_t* counter = nullptr;
+    uint64_t* ctrl_all_dev = nullptr;
+    uint64_t* ctrl_all_host = nullptr;
+    vr::LaunchCfg cfg{};
+    int kw = 1, tier = vr::kTierHash, blocks = 0;
+    int64_t total_tiles = 0;
+    int64_t total_rows = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t graph_stream = nullptr;  // the stream the graph was captured for
+};
+
+using namespace vr;
+
+static int batched_enqueue(vr_batched* b, cudaStream_t st) {
+    cudaError_t e;
+    const int n = (int)b->inst.size();
+    if (b->mode == VR_BATCHED_PERSISTENT) {
+        dim3 grid(148 * 2, std::min(b->num_spans, 65535));
+        k_zero_many<<<grid, 256, 0, st>>>(b->spans_dev, b->num_spans);
+        if ((e = cudaGetLastError()) != cudaSuccess) return VR_ERR_CUDA;
+        LaunchCfg L = b->cfg;
+        L.total_tiles = b->total_tiles;
+        L.num_desc = n;
+        if ((e = launch_aggregate(b->kw, b->tier, b->descs_dev, L, b->blocks, b->counter, st)) != cudaSuccess)
+            return VR_ERR_CUDA;
+    } else {
+        for (int i = 0; i < n; ++i) {
+            vr_agg* h = b->inst[i];
+            const BatchDesc& d = b->descs[i];
+            if ((e = cudaMemsetAsync(h->table, 0, (size_t)h->table_slots * h->plan.prog.sw * 8, st)) != cudaSuccess)
+                return VR_ERR_CUDA;
+            if ((e = cudaMemsetAsync(d.ctrl, 0, CTRL_WORDS * 8, st)) != cudaSuccess) return VR_ERR_CUDA;
+            LaunchCfg L = h->launch;
+            L.total_tiles = d.num_tiles;
+            int blocks = (int)std::min<int64_t>(h->blocks, d.num_tiles);
+            if ((e = launch_aggregate(h->plan.prog.kw, h->cfg.tier, b->descs_dev + i, L, blocks, &d.ctrl[CTRL_NEXT_TILE],
+                                      st)) != cudaSuccess)
+                return VR_ERR_CUDA;
+        }
+    }
+    k_gather_ctrl<<<(n * CTRL_WORDS + 255) / 256, 256, 0, st>>>(b->descs_dev, n, b->ctrl_all_dev);
+    if ((e = cudaGetLastError()) != cudaSuccess) return VR_ERR_CUDA;
+    if ((e = cudaMemcpyAsync(b->ctrl_all_host, b->ctrl_all_dev, (size_t)n * CTRL_WORDS * 8, cudaMemcpyDeviceToHost, st)) !=
+        cudaSuccess)
+        return VR_ERR_CUDA;
+    return VR_OK;
+}
+
+extern "C" {
+
+int vr_batched_create(const vr_batched_plan* plan, vr_batched** out) {
+    if (!plan || !out || plan->num_instances <= 0 || !plan->instances || !plan->batches) return VR_ERR_INVALID;
+    *out = nullptr;
+    vr_batched* b = new vr_batched();
+    b->mode = plan->mode;
+    b->use_graph = plan->use_graph != 0;
+    const int n = plan->num_instances;
+    vr_agg* h0 = plan->instances[0];
+    b->device = h0->device;
+    cudaSetDevice(b->device);
+    // every instance must share the program shape (one kernel, one stage layout)
+    int max_tier_bytes = 0;
+    for (int i = 0; i < n; ++i) {
+        vr_agg* h = plan->instances[i];
+        const vr_batch& bt = plan->batches[i];
+        if (!h || h->dead || bt.location != VR_DEVICE) {
+            delete b;
+            set_thread_error("batched instances need live handles and device-resident batches");
+            return VR_ERR_INVALID;
+        }
+        if (h->device != b->device || std::memcmp(&h->plan.prog, &h0->plan.prog, sizeof(Program)) != 0 ||
+            h->cfg.tier != h0->cfg.tier || h->cfg.tile_rows != h0->cfg.tile_rows || h->cfg.stages != h0->cfg.stages ||
+            h->cfg.threads != h0->cfg.threads) {
+            delete b;
+            set_thread_error("batched instances must share device, spec shape and block shape");
+            return VR_ERR_UNSUPPORTED;
+        }
+        if (vr_agg_sync(h) != VR_OK) {
+            delete b;
+            set_thread_error("instance handle failed");
+            return VR_ERR_STATE;
+        }
+        max_tier_bytes = std::max(max_tier_bytes, h->launch.tier_bytes);
+        b->inst.push_back(h);
+    }
+    b->kw = h0->plan.prog.kw;
+    b->tier = h0->cfg.tier;
+    b->cfg = h0->launch;
+    b->cfg.tier_bytes = max_tier_bytes;
+    b->cfg.smem_bytes = smem_map(b->cfg.stages, b->cfg.lay.stage_bytes, max_tier_bytes).total;
+    const DeviceInfo& di = device_info(b->device);
+    b->blocks = di.sms * ((2 * b->cfg.smem_bytes <= di.smem_optin) ? 2 : 1);
+    // descriptors: instance i's tiles follow instance i-1's
+    std::vector<ZeroSpan> spans;
+    int64_t tile = 0;
+    for (int i = 0; i < n; ++i) {
+        vr_agg* h = b->inst[i];
+        const vr_batch& bt = plan->batches[i];
+        StageSlot& s = h->slot[0];
+        if (h->cfg.tier != kTierDirect && s.deferred_cap < bt.num_rows) {
+            cudaFree(s.deferred);
+            cudaFree(s.deferred_tmp);
+            s.deferred_cap = std::max<int64_t>(bt.num_rows, 4096);
+            if (cudaMalloc(&s.deferred, (size_t)s.deferred_cap * 8) != cudaSuccess ||
+                cudaMalloc(&s.deferred_tmp, (size_t)s.deferred_cap * 8) != cudaSuccess) {
+                vr_batched_destroy(b);
+                return VR_ERR_OOM;
+            }
+        }
+        BatchDesc d;
+        std::memset(&d, 0, sizeof(d));
+        for (int c = 0; c < h->plan.prog.num_cols; ++c) {
+            const vr_column& col = bt.columns[h->plan.spec_of_staged[c]];
+            d.col_data[c] = (const char*)col.data;
+            d.col_valid[c] = (const uint32_t*)col.validity;
+        }
+        d.selection = (const uint32_t*)bt.selection;
+        fill_desc(h, bt, d, s.ctrl_dev, s, b->mode == VR_BATCHED_PERSISTENT ? tile : 0);
+        bool tma = h->cfg.tma != 0;
+        for (int c = 0; c < h->plan.prog.num_cols; ++c)
+            tma = tma && ((uintptr_t)d.col_data[c] & 15) == 0 && ((uintptr_t)d.col_valid[c] & 15) == 0;
+        d.tma = tma && ((uintptr_t)d.selection & 15) == 0;
+        s.launched = d;
+        b->descs.push_back(d);
+        tile += d.num_tiles;
+        b->total_rows += bt.num_rows;
+        spans.push_back(ZeroSpan{h->table, h->table_slots * h->plan.prog.sw});
+        spans.push_back(ZeroSpan{s.ctrl_dev, CTRL_WORDS});
+    }
+    b->total_tiles = tile;
+    cudaError_t e;
+    spans.push_back(ZeroSpan{nullptr, 0});
+    b->num_spans = (int)spans.size() - 1;
+    if ((e = cudaMalloc(&b->descs_dev, sizeof(BatchDesc) * n)) != cudaSuccess ||
+        (e = cudaMalloc(&b->spans_dev, sizeof(ZeroSpan) * spans.size())) != cudaSuccess ||
+        (e = cudaMalloc(&b->counter, 64)) != cudaSuccess ||
+        (e = cudaMalloc(&b->ctrl_all_dev, (size_t)n * CTRL_WORDS * 8)) != cudaSuccess ||
+        (e = cudaMallocHost(&b->ctrl_all_host, (size_t)n * CTRL_WORDS * 8)) != cudaSuccess) {
+        vr_batched_destroy(b);
+        return VR_ERR_OOM;
+    }
+    // the tile counter is zeroed with the tables
+    b->num_spans += 1;
+    spans[spans.size() - 1] = ZeroSpan{b->counter, 8};
+    cudaMemcpy(b->descs_dev, b->descs.data(), sizeof(BatchDesc) * n, cudaMemcpyHostToDevice);
+    cudaMemcpy(b->spans_dev, spans.data(), sizeof(ZeroSpan) * spans.size(), cudaMemcpyHostToDevice);
+    *out = b;
+    return VR_OK;
+}
+
+int vr_batched_run(vr_batched* b, void* stream) {
+    if (!b) return VR_ERR_INVALID;
+    cudaSetDevice(b->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e;
+    int rc;
+    if (b->use_graph) {
+        if (!b->exec || b->graph_stream != st) {
+            if (b->exec) cudaGraphExecDestroy(b->exec);
+            if (b->graph) cudaGraphDestroy(b->graph);
+            b->exec = nullptr;
+            b->graph = nullptr;
+            cudaStream_t cap = st;
+            bool own = false;
+            if (!cap) {  // the legacy stream cannot be captured
+                cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
+                own = true;
+            }
+            if ((e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return VR_ERR_CUDA;
+            rc = batched_enqueue(b, cap);
+            e = cudaStreamEndCapture(cap, &b->graph);
+            if (own) cudaStreamDestroy(cap);
+            if (rc != VR_OK || e != cudaSuccess) return VR_ERR_CUDA;
+            if ((e = cudaGraphInstantiate(&b->exec, b->graph, 0)) != cudaSuccess) return VR_ERR_CUDA;
+            b->graph_stream = st;
+        }
+        if ((e = cudaGraphLaunch(b->exec, st)) != cudaSuccess) return VR_ERR_CUDA;
+    } else {
+        rc = batched_enqueue(b, st);
+        if (rc != VR_OK) return rc;
+    }
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return VR_ERR_CUDA;
+    // per-instance bookkeeping: groups, errors, and growth + replay where needed
+    const int n = (int)b->inst.size();
+    int status = VR_OK;
+    for (int i = 0; i < n; ++i) {
+        vr_agg* h = b->inst[i];
+        StageSlot& s = h->slot[0];
+        std::memcpy(s.ctrl_host, b->ctrl_all_host + (size_t)i * CTRL_WORDS, CTRL_WORDS * 8);
+        h->groups_known = 0;
+        h->compact_valid = false;
+        h->stats.rows += b->descs[i].num_rows;
+        h->stats.batches++;
+        h->stats.kernel_launches++;
+        s.launched = b->descs[i];
+        s.pending = true;
+        h->next_slot = 0;
+        int64_t old_cap = h->cfg.capacity;
+        int rc2 = agg_resolve_all(h);
+        if (rc2 != VR_OK && status == VR_OK) status = rc2;
+        if (h->cfg.capacity != old_cap) {  // grown: later runs use the new table
+            BatchDesc d = b->descs[i];
+            d.table = h->table;
+            d.cap_mask = h->cfg.capacity - 1;
+            b->descs[i] = d;
+            cudaMemcpy(b->descs_dev + i, &d, sizeof(BatchDesc), cudaMemcpyHostToDevice);
+            ZeroSpan zs{h->table, h->table_slots * h->plan.prog.sw};
+            cudaMemcpy(b->spans_dev + 2 * i, &zs, sizeof(ZeroSpan), cudaMemcpyHostToDevice);
+            if (b->exec) {  // the graph captured the old pointers in kernel arguments only via descs: still valid
+            }
+        }
+    }
+    return status;
+}
+
+void vr_batched_destroy(vr_batched* b) {
+    if (!b) return;
+    cudaSetDevice(b->device);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    cudaFree(b->descs_dev);
+    cudaFree(b->spans_dev);
+    cudaFree(b->counter);
+    cudaFree(b->ctrl_all_dev);
+    cudaFreeHost(b->ctrl_all_host);
+    delete b;
+}
+
+}  // extern "C"

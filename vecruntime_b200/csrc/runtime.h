@@ -1,0 +1,123 @@
+// Runtime state behind the C ABI: the aggregate handle, its device table,
+// staging, and the launch configuration. Shared by abi.cu, batched.cu,
+// tune.cpp and serving.cpp.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "agg_kernels.cuh"
+#include "plan.h"
+#include "vrgpu.h"
+
+namespace vr {
+
+// Launch configuration of one handle (chosen by the tuner or forced).
+struct Config {
+    int tier = kTierHash;
+    int warp_agg = 0;
+    int threads = 256;        // consumer threads
+    int blocks_per_sm = 1;
+    int tile_rows = 2048;
+    int stages = 2;
+    int smem_slots = 0;       // hash tier shared cache
+    int tma = 1;
+    int g_probes = 512;
+    int s_probes = 8;
+    int64_t capacity = 0;     // HBM table slots (hash tier: power of two)
+};
+
+// One staging set: a batch in flight (ping-pong between two).
+struct StageSlot {
+    char* dev = nullptr;        // staged host columns
+    size_t dev_cap = 0;
+    BatchDesc* desc_host = nullptr;  // pinned
+    BatchDesc* desc_dev = nullptr;
+    uint64_t* ctrl_dev = nullptr;
+    uint64_t* ctrl_host = nullptr;   // pinned mirror, copied after each launch
+    int64_t* deferred = nullptr;
+    int64_t* deferred_tmp = nullptr;
+    int64_t deferred_cap = 0;
+    uint64_t* spill = nullptr;
+    int64_t spill_cap = 0;
+    cudaEvent_t done = nullptr;
+    cudaEvent_t t0 = nullptr, t1 = nullptr;  // kernel timing (trace)
+    cudaEvent_t h0 = nullptr;                // H2D start (trace)
+    cudaEvent_t copied = nullptr;            // this slot's H2D copies are done
+    bool pending_done_recorded = false;      // `done` has been recorded at least once
+    BatchDesc launched{};             // host copy of the last launch's descriptor
+    bool pending = false;
+    bool timed = false;
+    bool staged_h2d = false;
+    int64_t rows = 0;
+};
+
+struct DeviceInfo {
+    int sms = 148;
+    int smem_optin = 232448;
+    bool ready = false;
+};
+DeviceInfo& device_info(int device);
+
+}  // namespace vr
+
+struct vr_agg {
+    int device = 0;
+    cudaStream_t stream = nullptr;       // kernels, emission
+    cudaStream_t copy_stream = nullptr;  // host -> device staging copies
+    bool own_stream = false;
+    // spec copy
+    std::vector<vr_column_type> columns;
+    std::vector<int32_t> keys;
+    std::vector<vr_agg_fn> fns;
+    vr_agg_spec spec{};
+    vr::Plan plan;
+    vr::Config cfg;
+    vr::LaunchCfg launch{};
+    int blocks = 0;
+    vr::Program* prog_dev = nullptr;
+    vr::EmitProgram* emit_dev = nullptr;
+    uint64_t* table = nullptr;
+    int64_t table_slots = 0;      // slots scanned by compaction (incl. the side slot)
+    vr::StageSlot slot[2];
+    int next_slot = 0;
+    int64_t groups_known = 0;
+    // compaction / emission
+    bool compact_valid = false;
+    int64_t* slot_of = nullptr;
+    int64_t slot_of_cap = 0;
+    int64_t* num_dev = nullptr;
+    int64_t num_groups = 0;
+    void* cub_temp = nullptr;
+    size_t cub_temp_bytes = 0;
+    vr_out_column* outs_dev = nullptr;
+    vr_out_column* outs_host = nullptr;  // pinned
+    char* emit_stage = nullptr;
+    size_t emit_stage_cap = 0;
+    uint64_t* emit_ctrl = nullptr;       // pinned mirror word
+    // descriptor + control block for rehash / emission (never a batch's)
+    vr::BatchDesc* aux_desc_host = nullptr;  // pinned
+    vr::BatchDesc* aux_desc_dev = nullptr;
+    uint64_t* aux_ctrl_dev = nullptr;
+    uint64_t* aux_ctrl_host = nullptr;       // pinned
+    // status
+    int status = VR_OK;
+    std::string last_error;
+    vr_agg_stats stats{};
+    bool trace = false;
+    bool dead = false;
+};
+
+namespace vr {
+// shared helpers (abi.cu)
+int set_err(vr_agg* h, int code, const std::string& msg);
+int cuda_err(vr_agg* h, cudaError_t e, const char* what);
+int agg_build(const vr_agg_spec* spec, const vr_tune_choice* forced, vr_agg** out, cudaStream_t stream);
+// Fills a BatchDesc for a device-resident batch (no copies).
+void fill_desc(vr_agg* h, const vr_batch& b, BatchDesc& d, uint64_t* ctrl, const StageSlot& s, int64_t tile_begin);
+int agg_resolve_all(vr_agg* h);
+int64_t tiles_for(const vr_agg* h, int64_t rows);
+void set_thread_error(const std::string& msg);
+}  // namespace vr
