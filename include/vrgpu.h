@@ -36,8 +36,10 @@
 #ifndef VRGPU_H
 #define VRGPU_H
 
+#ifndef __CUDACC_RTC__ /* per-spec kernels compiled at run time get these types from their prelude */
 #include <stddef.h>
 #include <stdint.h>
+#endif
 
 #ifdef __cplusplus
 extern "C" {
@@ -145,7 +147,9 @@ enum vr_spec_flags {
     VR_SPEC_NO_WARP_AGG = 8,   /* no __match_any_sync pre-aggregation            */
     VR_SPEC_WARP_AGG = 16,     /* force __match_any_sync pre-aggregation         */
     VR_SPEC_NO_TMA = 32,       /* plain loads instead of bulk copies into smem   */
-    VR_SPEC_TRACE = 64         /* record cudaEvent pairs per H2D / kernel / D2H  */
+    VR_SPEC_TRACE = 64,        /* record cudaEvent pairs per H2D / kernel / D2H  */
+    VR_SPEC_NO_JIT = 128       /* run the interpreted kernel, not one compiled
+                                  for this spec (also: environment VRGPU_JIT=0)  */
 };
 
 typedef struct vr_agg_spec {
@@ -202,6 +206,8 @@ typedef struct vr_agg_stats {
     double total_h2d_ms;
     double total_d2h_ms;
     int64_t kernel_launches;   /* every kernel this handle launched             */
+    int32_t jit;               /* 1: the aggregate kernel was compiled for this spec */
+    int32_t reserved;
 } vr_agg_stats;
 
 typedef struct vr_agg vr_agg;
@@ -315,6 +321,11 @@ typedef struct vr_plan_info {
     char reason[160];       /* why a spec was refused                              */
 } vr_plan_info;
 int vr_agg_plan(const vr_agg_spec* spec, vr_plan_info* info, vr_column_type* out_types, int32_t cap);
+
+/* Compiles the spec's specialised aggregate kernel for `tier` (0 direct,
+ * 1 hash) with NVRTC -- host only, no GPU needed -- and reports the cubin
+ * size; on failure the compiler log goes to `log`. */
+int vr_jit_compile(const vr_agg_spec* spec, int32_t tier, int64_t* cubin_bytes, char* log, size_t cap);
 /* 1 and the recorded choice when the tuner has one for (spec, rows), else 0. */
 int vr_tune_lookup(const vr_agg_spec* spec, int64_t rows, vr_tune_choice* out);
 int vr_tune_record(const vr_agg_spec* spec, int64_t rows, const vr_tune_choice* choice, double rows_per_s);

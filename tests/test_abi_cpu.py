@@ -112,3 +112,20 @@ def test_create_without_gpu_fails_loudly():
     cols = [vr.longs(np.zeros(1, np.int64), nullable=False)]
     with pytest.raises(vr.VrError):
         vr.GpuHashAggregate(cols, [0], [vr.CountAgg()])
+
+
+@pytest.mark.parametrize("workload,tier", [("decimal_report", 0), ("plain", 1)])
+def test_jit_specialises_the_aggregate_kernel_without_a_gpu(workload, tier):
+    """NVRTC compiles the per-spec aggregate kernel for sm_100a on the host;
+    the same source the runtime launches, so a compile error shows here."""
+    from vecruntime_b200 import datagen as G
+
+    w = getattr(G, workload)(rows=1000)
+    sp = w.spec()
+    log = C.create_string_buffer(8192)
+    nbytes = C.c_int64()
+    rc = N.lib().vr_jit_compile(C.byref(sp.spec), tier, C.byref(nbytes), log, len(log))
+    if rc == N.VR_ERR_UNSUPPORTED and b"nvrtc" in log.value.lower():
+        pytest.skip("libnvrtc is not loadable here: " + log.value.decode())
+    assert rc == N.VR_OK, log.value.decode()
+    assert nbytes.value > 10_000

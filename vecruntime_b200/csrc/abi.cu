@@ -15,6 +15,7 @@
 #include <string>
 
 #include "runtime.h"
+#include "jit.h"
 #include "tune.h"
 
 namespace vr {
@@ -53,7 +54,6 @@ DeviceInfo& device_info(int device) {
         cudaSetDevice(device);
         cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, device);
         cudaDeviceGetAttribute(&d.smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
-        upload_pow10();
         cudaSetDevice(prev);
         d.ready = true;
     }
@@ -100,6 +100,14 @@ static void fill_layout(const Program& P, int T, StageLayout& L) {
 
 int64_t tiles_for(const vr_agg* h, int64_t rows) { return (rows + h->cfg.tile_rows - 1) / h->cfg.tile_rows; }
 
+// The aggregate launch: the spec's own kernel when it was compiled, else the
+// interpreted ahead-of-time one.
+cudaError_t agg_launch(vr_agg* h, const BatchDesc* descs, const LaunchCfg& L, int blocks, uint64_t* tile_counter,
+                       cudaStream_t st) {
+    if (h->jit) return jit_launch(h->jit, descs, L, blocks, tile_counter, st);
+    return launch_aggregate(h->plan.prog.kw, h->cfg.tier, descs, L, blocks, tile_counter, st);
+}
+
 // Picks tier, block shape, tile and shared-cache sizes. `forced` (tests /
 // tuner) overrides the defaults field by field.
 static int choose_config(vr_agg* h, const vr_tune_choice* forced) {
@@ -126,7 +134,8 @@ static int choose_config(vr_agg* h, const vr_tune_choice* forced) {
         const int Ts[] = {2048, 1024, 512};
         for (int nt : nts) {
             if (forced && forced->threads && nt != forced->threads) continue;
-            int64_t tb = P.direct_slots * P.aw * (int64_t)nt * 8;
+            // thread-private hot words + the CTA's cold words
+            int64_t tb = (P.direct_slots * P.hw * (int64_t)nt + P.direct_slots * P.aw) * 8;
             if (tb > budget) continue;
             for (int T : Ts) {
                 if (forced && forced->tile_rows && T != forced->tile_rows) continue;
@@ -177,10 +186,15 @@ static int choose_config(vr_agg* h, const vr_tune_choice* forced) {
     if (fl & VR_SPEC_NO_WARP_AGG) c.warp_agg = 0;
     if (forced) c.warp_agg = forced->warp_agg;
     if (fl & VR_SPEC_NO_TMA) c.tma = 0;
-    const int tier_bytes = c.tier == kTierDirect ? (int)(P.direct_slots * P.aw * (int64_t)c.threads * 8)
-                                                 : c.smem_slots * P.sw * 8;
+    const int tier_bytes = c.tier == kTierDirect
+                               ? (int)((P.direct_slots * P.hw * (int64_t)c.threads + P.direct_slots * P.aw) * 8)
+                               : c.smem_slots * P.sw * 8;
     SmemMap m = smem_map(c.stages, stage_bytes_for(P, c.tile_rows), tier_bytes);
+    // blocks per SM: shared memory and registers (the ahead-of-time kernel's;
+    // refined once a per-spec kernel is loaded)
     c.blocks_per_sm = (2 * m.total <= budget) ? 2 : 1;
+    int regs = aggregate_kernel_regs(P.kw, c.tier);
+    if (regs > 0 && 2 * ((regs + 7) / 8 * 8) * (c.threads + 32) > 65536) c.blocks_per_sm = 1;
     if (forced && forced->blocks_per_sm) c.blocks_per_sm = forced->blocks_per_sm;
     if (m.total > budget) return set_err(h, VR_ERR_UNSUPPORTED, "configuration exceeds shared memory");
     if (c.threads % 32 || c.threads > kMaxConsumerThreads || c.tile_rows % 128)
@@ -308,6 +322,24 @@ int agg_build(const vr_agg_spec* spec, const vr_tune_choice* forced, vr_agg** ou
     h->stats.blocks = h->blocks;
     h->stats.smem_bytes = h->launch.smem_bytes;
     h->stats.tile_rows = h->cfg.tile_rows;
+    // the spec's own kernel (compiled once per process per spec); the
+    // interpreted ahead-of-time kernel stays the fallback
+    if (jit_enabled() && !(spec->flags & VR_SPEC_NO_JIT)) {
+        std::string why;
+        h->jit = jit_get(h->plan.prog, h->plan.prog.kw, h->cfg.tier, h->device, &why);
+        if (h->jit) {
+            int regs = jit_regs(h->jit);
+            const DeviceInfo& di = device_info(h->device);
+            int bps = (2 * h->launch.smem_bytes <= di.smem_optin) ? 2 : 1;
+            if (2 * ((regs + 7) / 8 * 8) * (h->cfg.threads + 32) > 65536) bps = 1;
+            h->cfg.blocks_per_sm = bps;
+            h->blocks = di.sms * bps;
+            h->stats.blocks = h->blocks;
+        } else {
+            h->jit_error = why;
+        }
+    }
+    h->stats.jit = h->jit ? 1 : 0;
     if ((e = cudaMalloc(&h->prog_dev, sizeof(Program))) != cudaSuccess ||
         (e = cudaMalloc(&h->emit_dev, sizeof(EmitProgram))) != cudaSuccess ||
         (e = cudaMemcpy(h->prog_dev, &h->plan.prog, sizeof(Program), cudaMemcpyHostToDevice)) != cudaSuccess ||
@@ -648,8 +680,7 @@ static int agg_update(vr_agg* h, const vr_batch* b) {
     L.total_tiles = d.num_tiles;
     int blocks = (int)std::min<int64_t>(h->blocks, d.num_tiles);
     if (h->trace) cudaEventRecord(s.t0, h->stream);
-    if ((e = launch_aggregate(h->plan.prog.kw, h->cfg.tier, s.desc_dev, L, blocks, &s.ctrl_dev[CTRL_NEXT_TILE],
-                              h->stream)) != cudaSuccess)
+    if ((e = agg_launch(h, s.desc_dev, L, blocks, &s.ctrl_dev[CTRL_NEXT_TILE], h->stream)) != cudaSuccess)
         return cuda_err(h, e, "aggregate launch");
     if (h->trace) {
         cudaEventRecord(s.t1, h->stream);
@@ -963,6 +994,22 @@ int vr_hash_rows(int32_t num_keys, const vr_column_type* types, const vr_column*
         return VR_ERR_CUDA;
     }
     return VR_OK;
+}
+
+int vr_jit_compile(const vr_agg_spec* spec, int32_t tier, int64_t* cubin_bytes, char* log, size_t cap) {
+    if (!spec) return VR_ERR_INVALID;
+    Plan plan;
+    int rc = compile_plan(*spec, plan);
+    if (rc != VR_OK) {
+        if (log && cap) std::snprintf(log, cap, "%s", plan.reason.c_str());
+        return rc;
+    }
+    size_t bytes = 0;
+    std::string err;
+    bool ok = jit_compile_only(plan.prog, plan.prog.kw, tier == 0 ? kTierDirect : kTierHash, &bytes, &err);
+    if (log && cap) std::snprintf(log, cap, "%s", err.c_str());
+    if (cubin_bytes) *cubin_bytes = (int64_t)bytes;
+    return ok ? VR_OK : VR_ERR_UNSUPPORTED;
 }
 
 int vr_agg_plan(const vr_agg_spec* spec, vr_plan_info* info, vr_column_type* out_types, int32_t cap) {

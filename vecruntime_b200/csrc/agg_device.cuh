@@ -13,8 +13,10 @@
 //   LongMinMax / DoubleMinMax / Decimal128MinMax :1203-1462 -> OP_MAX_KEY / OP_MAX_D128
 // with Spark's NaN ordering (CompareOp.java:68-81, AggKernels.java:40-41).
 #pragma once
+#ifndef __CUDACC_RTC__
 #include <cuda_runtime.h>
 #include <stdint.h>
+#endif
 
 #include "vr_internal.h"
 
@@ -22,10 +24,23 @@ namespace vr {
 
 #define VR_DEV __device__ __forceinline__
 
+// Per-spec compilation (NVRTC, jit.cpp) defines VR_JIT and a compile-time
+// constant Program kJitProg: the program is then read from it (folded into
+// the code) instead of from the shared-memory copy, and loops over ops and
+// key fields unroll completely.
+#ifdef VR_JIT
+#define VR_PROG(smem_copy) (kJitProg)
+#define VR_UNROLL _Pragma("unroll")
+#else
+#define VR_PROG(smem_copy) (*reinterpret_cast<const Program*>(smem_copy))
+#define VR_UNROLL
+#endif
+
 constexpr uint32_t kFull = 0xffffffffu;
 // Spin limits: every wait in these kernels gives up after this many polls and
 // reports kErrTimeout / kErrLockTimeout instead of hanging the device.
-constexpr uint32_t kWaitPolls = 1u << 24;
+constexpr uint32_t kWaitPolls = 1u << 14;
+constexpr uint32_t kSuspendHintNs = 1000000;  // 1 ms per poll
 constexpr uint32_t kLockPolls = 1u << 22;
 // Single 64-bit keys are stored xor this constant so that 0 means "empty";
 // the one key equal to it lives in an extra slot past the table's end.
@@ -50,18 +65,22 @@ VR_DEV void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
         "r"(bytes)
         : "memory");
 }
+// try_wait with a suspend-time hint: the thread sleeps until the phase
+// completes (or the hint, in ns, runs out) instead of spinning, so waiting
+// warps leave the issue slots to the warps doing work.
 VR_DEV bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(kSuspendHintNs)
         : "memory");
     return ok != 0;
 }
-// Bounded wait: false when the poll budget ran out.
+// Bounded wait: false when the poll budget ran out (kWaitPolls suspended
+// polls of up to kSuspendHintNs each: seconds, never forever).
 VR_DEV bool mbar_wait(uint64_t* bar, uint32_t parity) {
     for (uint32_t i = 0; i < kWaitPolls; ++i)
         if (mbar_try_wait(bar, parity)) return true;
@@ -258,9 +277,29 @@ VR_DEV bool mul_i128_i64(I128 a, int64_t b, I128& out) {
     return true;
 }
 
-// 10^p for p in [0, 38] as (lo, hi) words, uploaded once per device.
-__constant__ uint64_t c_pow10_lo[39];
-__constant__ uint64_t c_pow10_hi[39];
+// 10^p for p in [0, 38] as (lo, hi) words, built by the compiler so every
+// module (the prebuilt one and each per-spec one) carries its own copy.
+struct Pow10Table {
+    uint64_t lo[39];
+    uint64_t hi[39];
+};
+
+constexpr Pow10Table make_pow10_table() {
+    Pow10Table t{};
+    uint64_t lo = 1, hi = 0;
+    for (int i = 0; i < 39; ++i) {
+        t.lo[i] = lo;
+        t.hi[i] = hi;
+        // (hi, lo) *= 10 in 32-bit halves so no 128-bit type is needed
+        uint64_t a = (lo & 0xffffffffull) * 10;
+        uint64_t b = (lo >> 32) * 10 + (a >> 32);
+        lo = (b << 32) | (a & 0xffffffffull);
+        hi = hi * 10 + (b >> 32);
+    }
+    return t;
+}
+
+__constant__ const Pow10Table c_pow10 = make_pow10_table();
 
 // |v| < 10^p for a signed 128-bit v (lo, hi).
 VR_DEV bool within_precision(uint64_t lo, int64_t hi, int p) {
@@ -269,7 +308,7 @@ VR_DEV bool within_precision(uint64_t lo, int64_t hi, int p) {
         mlo = ~lo + 1;
         mhi = ~(uint64_t)hi + (mlo == 0 ? 1 : 0);
     }
-    uint64_t plo = c_pow10_lo[p], phi = c_pow10_hi[p];
+    uint64_t plo = c_pow10.lo[p], phi = c_pow10.hi[p];
     return mhi < phi || (mhi == phi && mlo < plo);
 }
 
@@ -312,52 +351,148 @@ VR_DEV int64_t ld_int(const TileView& v, int c, int lane, int64_t r) {
     return lane == VR_INT32 || lane == VR_DICT32 ? (int64_t)ld_i32(v, c, r) : ld_i64(v, c, r);
 }
 
+// The columns one op reads, with their pointers in registers: built once per
+// op per chunk of rows, so the per-row loop reloads nothing from the tile
+// header after a store. Column c of the op is 0 (input / first factor),
+// 1 (second buffer / factor) or 2 (third factor).
+struct OpView {
+    const char* d0;
+    const char* d1;
+    const char* d2;
+    const uint32_t* v0;
+    const uint32_t* v1;
+    const uint32_t* v2;
+};
+VR_DEV const char* vdata(const TileView& v, int c) { return v.data[c]; }
+VR_DEV const char* vdata(const OpView& v, int c) { return c == 0 ? v.d0 : c == 1 ? v.d1 : v.d2; }
+VR_DEV const uint32_t* vvalid(const OpView& v, int c) { return c == 0 ? v.v0 : c == 1 ? v.v1 : v.v2; }
+VR_DEV bool col_valid(const OpView& v, int c, int64_t r) {
+    const uint32_t* w = vvalid(v, c);
+    return w == nullptr || bit_at(w, r);
+}
+VR_DEV int32_t ld_i32(const OpView& v, int c, int64_t r) { return reinterpret_cast<const int32_t*>(vdata(v, c))[r]; }
+VR_DEV int64_t ld_i64(const OpView& v, int c, int64_t r) { return reinterpret_cast<const int64_t*>(vdata(v, c))[r]; }
+VR_DEV double ld_f64(const OpView& v, int c, int64_t r) { return reinterpret_cast<const double*>(vdata(v, c))[r]; }
+VR_DEV I128 ld_d128(const OpView& v, int c, int64_t r) {
+    const uint64_t* p = reinterpret_cast<const uint64_t*>(vdata(v, c)) + 2 * r;
+    I128 x;
+    x.lo = p[0];
+    x.hi = (int64_t)p[1];
+    return x;
+}
+VR_DEV int64_t ld_int(const OpView& v, int c, int lane, int64_t r) {
+    return lane == VR_INT32 || lane == VR_DICT32 ? (int64_t)ld_i32(v, c, r) : ld_i64(v, c, r);
+}
+
+// The op's columns from a tile view; `oo` is `o` with its column indices
+// renumbered to the view's 0..2.
+VR_DEV void make_opview(const OpDesc& o, const TileView& v, OpDesc& oo, OpView& ov) {
+    oo = o;
+    ov.d0 = ov.d1 = ov.d2 = nullptr;
+    ov.v0 = ov.v1 = ov.v2 = nullptr;
+    if (o.nterms > 0) {
+        ov.d0 = v.data[o.term_col[0]];
+        ov.v0 = v.valid[o.term_col[0]];
+        ov.d1 = v.data[o.term_col[1]];
+        ov.v1 = v.valid[o.term_col[1]];
+        if (o.nterms > 2) {
+            ov.d2 = v.data[o.term_col[2]];
+            ov.v2 = v.valid[o.term_col[2]];
+        }
+        oo.term_col[0] = 0;
+        oo.term_col[1] = 1;
+        oo.term_col[2] = 2;
+    } else if (o.col >= 0) {
+        ov.d0 = v.data[o.col];
+        ov.v0 = v.valid[o.col];
+        oo.col = 0;
+        if (o.col2 >= 0) {
+            ov.d1 = v.data[o.col2];
+            ov.v1 = v.valid[o.col2];
+            oo.col2 = 1;
+        }
+    }
+}
+
 // ------------------------------------------------------ key packing ----
+// k[idx] |= v with a runtime idx, without indexing the array at run time
+// (which would place it in local memory).
+template <int KW>
+VR_DEV void or_word(uint64_t (&k)[KW], int idx, uint64_t v) {
+#pragma unroll
+    for (int i = 0; i < KW; ++i)
+        if (i == idx) k[i] |= v;
+}
+
 // Packs row r's key tuple into KW words; `side` is set for the one single
 // 64-bit key equal to kSentinel (sentinel layout only). Null keys store zero
 // data and their null bit, as GroupKeyTable.insert does (GroupKeyTable.java:2515-2540).
+// One key field of row r into the packed words (null: its null bit only).
+template <int KW>
+VR_DEV void pack_field(const KeyField& kf, const TileView& v, int64_t r, uint64_t (&k)[KW], bool& bad) {
+    if (!col_valid(v, kf.col, r)) {
+        if (kf.null_word >= 0) or_word<KW>(k, kf.null_word, 1ull << kf.null_shift);
+        return;
+    }
+    switch (kf.lane) {
+        case VR_INT32:
+        case VR_DICT32: {
+            uint32_t u = (uint32_t)ld_i32(v, kf.col, r);
+            if (kf.bits < 32 && (u >> kf.bits) != 0) bad = true;  // id outside the declared dictionary
+            or_word<KW>(k, kf.word, (uint64_t)u << kf.shift);
+            break;
+        }
+        case VR_INT64:
+        case VR_FLOAT64:
+            or_word<KW>(k, kf.word, ld_u64(v, kf.col, r));
+            break;
+        case VR_BOOL:
+            or_word<KW>(k, kf.word, (uint64_t)bit_at(reinterpret_cast<const uint32_t*>(v.data[kf.col]), r) << kf.shift);
+            break;
+        case VR_DECIMAL128: {
+            I128 x = ld_d128(v, kf.col, r);
+            or_word<KW>(k, kf.word, x.lo);
+            or_word<KW>(k, kf.word + 1, (uint64_t)x.hi);
+            break;
+        }
+    }
+}
+
+// The occupancy bit, or (sentinel layout: one 64-bit word, no spare bit) the
+// xor with kSentinel and the side-slot test.
+template <int KW>
+VR_DEV void pack_finish(int occ_word, int occ_shift, uint64_t (&k)[KW], bool& side) {
+    if (occ_word >= 0) {
+        or_word<KW>(k, occ_word, 1ull << occ_shift);
+    } else {
+        side = (k[0] == kSentinel);
+        k[0] ^= kSentinel;
+    }
+}
+
 template <int KW>
 VR_DEV void pack_key(const Program& P, const TileView& v, int64_t r, uint64_t (&k)[KW], bool& side, bool& bad) {
 #pragma unroll
     for (int i = 0; i < KW; ++i) k[i] = 0;
     side = false;
     bad = false;
-    for (int f = 0; f < P.num_keys; ++f) {
-        const KeyField& kf = P.keys[f];
-        bool ok = col_valid(v, kf.col, r);
-        if (!ok) {
-            if (kf.null_word >= 0) k[kf.null_word] |= 1ull << kf.null_shift;
-            continue;
-        }
-        switch (kf.lane) {
-            case VR_INT32:
-            case VR_DICT32: {
-                uint32_t u = (uint32_t)ld_i32(v, kf.col, r);
-                if (kf.bits < 32 && (u >> kf.bits) != 0) bad = true;  // id outside the declared dictionary
-                k[kf.word] |= (uint64_t)u << kf.shift;
-                break;
-            }
-            case VR_INT64:
-            case VR_FLOAT64:
-                k[kf.word] |= ld_u64(v, kf.col, r);
-                break;
-            case VR_BOOL:
-                k[kf.word] |= (uint64_t)bit_at(reinterpret_cast<const uint32_t*>(v.data[kf.col]), r) << kf.shift;
-                break;
-            case VR_DECIMAL128: {
-                I128 x = ld_d128(v, kf.col, r);
-                k[kf.word] |= x.lo;
-                if (kf.word + 1 < KW) k[kf.word + 1] |= (uint64_t)x.hi;
-                break;
-            }
-        }
+    for (int f = 0; f < P.num_keys; ++f) pack_field<KW>(P.keys[f], v, r, k, bad);
+    pack_finish<KW>(P.occ_word, P.occ_shift, k, side);
+}
+
+// Direct tier: one field's share of the combination index; -1 when its id
+// lies outside the declared dictionary (null is the field's last value).
+VR_DEV int64_t direct_field(const KeyField& kf, const TileView& v, int64_t r) {
+    int64_t val;
+    if (!col_valid(v, kf.col, r)) {
+        val = kf.card - 1;
+    } else if (kf.lane == VR_BOOL) {
+        val = bit_at(reinterpret_cast<const uint32_t*>(v.data[kf.col]), r);
+    } else {
+        val = (int64_t)(uint32_t)ld_i32(v, kf.col, r);
+        if (val >= (int64_t)kf.card - (kf.null_word >= 0 ? 1 : 0)) return -1;
     }
-    if (P.occ_word >= 0) {
-        k[P.occ_word] |= 1ull << P.occ_shift;
-    } else {  // sentinel layout: one 64-bit word, no spare bit
-        side = (k[0] == kSentinel);
-        k[0] ^= kSentinel;
-    }
+    return val * kf.mul;
 }
 
 // Direct tier: the combination index of a row's dictionary / boolean keys;
@@ -365,17 +500,9 @@ VR_DEV void pack_key(const Program& P, const TileView& v, int64_t r, uint64_t (&
 VR_DEV int64_t direct_index(const Program& P, const TileView& v, int64_t r) {
     int64_t idx = 0;
     for (int f = 0; f < P.num_keys; ++f) {
-        const KeyField& kf = P.keys[f];
-        int64_t val;
-        if (!col_valid(v, kf.col, r)) {
-            val = kf.card - 1;  // null is the last value of a nullable field
-        } else if (kf.lane == VR_BOOL) {
-            val = bit_at(reinterpret_cast<const uint32_t*>(v.data[kf.col]), r);
-        } else {
-            val = (int64_t)(uint32_t)ld_i32(v, kf.col, r);
-            if (val >= (int64_t)kf.card - (kf.null_word >= 0 ? 1 : 0)) return -1;  // id outside the dictionary
-        }
-        idx += val * kf.mul;
+        int64_t x = direct_field(P.keys[f], v, r);
+        if (x < 0) return -1;
+        idx += x;
     }
     return idx;
 }
@@ -466,159 +593,205 @@ VR_DEV uint64_t* find_or_insert(uint64_t* table, int64_t mask, int sw, const uin
 }
 
 // ----------------------------------------------------- contributions ----
-// One row's (or one warp's peers') contribution to an op: up to kMaxContrib
-// words in the op's accumulator representation. All-zero == identity.
+// One row's contribution to an op, held in registers: the eight words are
+// named fields and are only ever addressed statically (an array indexed by a
+// runtime word count would live in local memory, which with most of L1
+// carved out for shared memory goes to L2).
+//
+// Three representations (words relative to the op's first word):
+//   raw     - values as read from the row (op_raw);
+//   global  - the shared/HBM table words: carry-save limbs that add exactly
+//             with 64-bit atomics, in any order (raw_to_global);
+//   private - the direct tier's thread-private words: running 64/128-bit sums
+//             plus a wrap count, so a sum touches one or two words per row.
+// kind         global words                           private words
+// COUNT_*      a=count                                a=count
+// SUM_I32      a=sum                                  a=sum
+// SUM_I64      a=sum lo32 (u) b=sum hi32 (s)          a=int64 sum  b=wraps
+// SUM_F64      a=sum b=compensation                   a=sum b=compensation
+// SUM_D128     a..d=32-bit limbs (d signed)           a,b=int128 sum  c=wraps
+// SUM_PROD     a,b=cs  c..f=limbs  g=ANSI flag        a=int64 sum b=wraps c,d=int128 e=wraps
+//              h=null products                        g=flag h=null products
+// MAX_KEY      a                                      a
+// MAX_D128     a=lo b=hi                              a=lo b=hi
+// MERGE_DSUM   a..d=limbs e=flags                     a,b=int128 c=wraps e=flags
+// MERGE_DAVG   a..d=limbs e,f=count cs g=flags        a,b=int128 c=wraps e=count f=wraps g=flags
 struct Contrib {
-    uint64_t w[kMaxContrib];
+    uint64_t a, b, c, d, e, f, g, h;
 };
 
-// A row is "live" when it is inside the tile, selected and has a slot.
-// Computes op `o`'s contribution of row r; returns false when the row adds
-// nothing (invalid input), leaving c zeroed.
-VR_DEV bool op_contrib(const OpDesc& o, const TileView& v, int64_t r, Contrib& c) {
-#pragma unroll
-    for (int i = 0; i < kMaxContrib; ++i) c.w[i] = 0;
-    switch (o.kind) {
+VR_DEV void czero(Contrib& x) { x.a = x.b = x.c = x.d = x.e = x.f = x.g = x.h = 0; }
+VR_DEV uint64_t lo32(int64_t x) { return (uint64_t)(uint32_t)x; }
+VR_DEV uint64_t hi32(int64_t x) { return (uint64_t)(int64_t)(int32_t)(x >> 32); }
+
+template <class V>
+VR_DEV bool terms_valid(const OpDesc& o, const V& v, int64_t r) {
+    bool ok = col_valid(v, o.term_col[0], r) && col_valid(v, o.term_col[1], r);
+    if (o.nterms > 2) ok = ok && col_valid(v, o.term_col[2], r);
+    return ok;
+}
+
+template <class V>
+VR_DEV int64_t term_value(const OpDesc& o, const V& v, int64_t r, int t) {
+    int64_t x = ld_i64(v, o.term_col[t], r);
+    return o.term_add[t] + (o.term_sign[t] < 0 ? -x : x);
+}
+
+// Raw values of row r for op o; false when the row contributes nothing.
+template <int K, class V>
+VR_DEV bool op_raw(const OpDesc& o, const V& v, int64_t r, Contrib& x) {
+    czero(x);
+    switch (K) {
         case OP_COUNT_ROWS:
-            c.w[0] = 1;
+            x.a = 1;
             return true;
         case OP_COUNT_VALID: {
-            bool ok = true;
-            if (o.nterms > 0) {
-                for (int t = 0; t < o.nterms; ++t) ok &= col_valid(v, o.term_col[t], r);
-            } else {
-                ok = col_valid(v, o.col, r);
-            }
-            c.w[0] = ok ? 1 : 0;
+            bool ok = o.nterms > 0 ? terms_valid(o, v, r) : col_valid(v, o.col, r);
+            x.a = ok ? 1 : 0;
             return ok;
         }
-        case OP_SUM_I32: {
+        case OP_SUM_I32:
             if (!col_valid(v, o.col, r)) return false;
-            c.w[0] = (uint64_t)(int64_t)ld_i32(v, o.col, r);
+            x.a = (uint64_t)(int64_t)ld_i32(v, o.col, r);
             return true;
-        }
-        case OP_SUM_I64: {
+        case OP_SUM_I64:
             if (!col_valid(v, o.col, r)) return false;
-            int64_t x = ld_int(v, o.col, o.lane, r);
-            c.w[0] = (uint64_t)(uint32_t)x;
-            c.w[1] = (uint64_t)(int64_t)(int32_t)(x >> 32);
+            x.a = (uint64_t)ld_int(v, o.col, o.lane, r);
             return true;
-        }
-        case OP_SUM_F64: {
+        case OP_SUM_F64:
             if (!col_valid(v, o.col, r)) return false;
-            double x = ld_f64(v, o.col, r);
-            c.w[0] = (uint64_t)__double_as_longlong(x);
-            c.w[1] = 0;  // +0.0
+            x.a = (uint64_t)__double_as_longlong(ld_f64(v, o.col, r));
             return true;
-        }
         case OP_SUM_D128: {
             if (!col_valid(v, o.col, r)) return false;
-            I128 x = ld_d128(v, o.col, r);
-            c.w[0] = (uint32_t)x.lo;
-            c.w[1] = (uint32_t)(x.lo >> 32);
-            c.w[2] = (uint32_t)(uint64_t)x.hi;
-            c.w[3] = (uint64_t)(int64_t)(int32_t)(x.hi >> 32);
+            I128 d = ld_d128(v, o.col, r);
+            x.a = d.lo;
+            x.b = (uint64_t)d.hi;
             return true;
         }
         case OP_SUM_PROD: {
-            bool ok = true;
-            for (int t = 0; t < o.nterms; ++t) ok &= col_valid(v, o.term_col[t], r);
-            if (!ok) return false;
-            // term values: addend + sign * column (INT64 unscaled lanes)
-            int64_t t0 = o.term_add[0] + (o.term_sign[0] < 0 ? -ld_i64(v, o.term_col[0], r) : ld_i64(v, o.term_col[0], r));
-            int64_t t1 = o.term_add[1] + (o.term_sign[1] < 0 ? -ld_i64(v, o.term_col[1], r) : ld_i64(v, o.term_col[1], r));
-            I128 p = mul_i64(t0, t1);
+            if (!terms_valid(o, v, r)) {
+                x.h = 1;  // a null factor: the product is null
+                return true;
+            }
+            I128 p = mul_i64(term_value(o, v, r, 0), term_value(o, v, r, 1));
             bool fits = true;
             if (o.nterms == 3) {
-                int64_t t2 = o.term_add[2] +
-                             (o.term_sign[2] < 0 ? -ld_i64(v, o.term_col[2], r) : ld_i64(v, o.term_col[2], r));
                 I128 q;
-                fits = mul_i128_i64(p, t2, q);
+                fits = mul_i128_i64(p, term_value(o, v, r, 2), q);
                 p = q;
             }
             if (!fits || !within_precision(p.lo, p.hi, o.prec)) {
                 // Spark's CheckOverflow on the product: null (non-ANSI) or an error (ANSI)
-                if (o.flags & OPF_CHECKED) c.w[6] = 1;
-                return (o.flags & OPF_CHECKED) != 0;
+                x.h = 1;
+                if (o.flags & OPF_CHECKED) x.g = 1;
+                return true;
             }
-            c.w[7] = 1;  // the row counts toward the sum (its product is not null)
-            bool small = (p.hi == ((int64_t)p.lo >> 63));
-            if (small) {
-                int64_t x = (int64_t)p.lo;
-                c.w[0] = (uint64_t)(uint32_t)x;
-                c.w[1] = (uint64_t)(int64_t)(int32_t)(x >> 32);
+            if (p.hi == ((int64_t)p.lo >> 63)) {
+                x.a = p.lo;  // fits int64: the common case
             } else {
-                c.w[2] = (uint32_t)p.lo;
-                c.w[3] = (uint32_t)(p.lo >> 32);
-                c.w[4] = (uint32_t)(uint64_t)p.hi;
-                c.w[5] = (uint64_t)(int64_t)(int32_t)(p.hi >> 32);
+                x.c = p.lo;
+                x.d = (uint64_t)p.hi;
+                x.e = 1;  // marks the 128-bit case in the raw form
             }
             return true;
         }
         case OP_MAX_KEY: {
             if (!col_valid(v, o.col, r)) return false;
             uint64_t k = o.lane == VR_FLOAT64 ? okey_f64(ld_f64(v, o.col, r)) : okey_i64(ld_int(v, o.col, o.lane, r));
-            c.w[0] = (o.flags & OPF_MIN) ? ~k : k;
+            x.a = (o.flags & OPF_MIN) ? ~k : k;
             return true;
         }
         case OP_MAX_D128: {
             if (!col_valid(v, o.col, r)) return false;
-            I128 x = ld_d128(v, o.col, r);
-            uint64_t lo = x.lo, hi = (uint64_t)x.hi ^ 0x8000000000000000ull;
+            I128 d = ld_d128(v, o.col, r);
+            uint64_t lo = d.lo, hi = (uint64_t)d.hi ^ 0x8000000000000000ull;
             if (o.flags & OPF_MIN) {
                 lo = ~lo;
                 hi = ~hi;
             }
-            c.w[0] = lo;
-            c.w[1] = hi;
+            x.a = lo;
+            x.b = hi;
             return true;
         }
         case OP_MERGE_DSUM: {
-            // WideDecimalSumMergeAgg.merge (VectorAggregates.scala:700-725): rows with a null or
-            // true isEmpty are skipped; a null sum on a non-empty row poisons the group.
-            const uint32_t* eb = reinterpret_cast<const uint32_t*>(v.data[o.col2]);
-            bool empty_valid = col_valid(v, o.col2, r);
-            if (!empty_valid || bit_at(eb, r)) return false;
+            // WideDecimalSumMergeAgg.merge (VectorAggregates.scala:700-725): rows whose isEmpty is
+            // null or true are skipped; a null sum on a non-empty row poisons the group.
+            if (!col_valid(v, o.col2, r) || bit_at(reinterpret_cast<const uint32_t*>(vdata(v, o.col2)), r)) return false;
             if (!col_valid(v, o.col, r)) {
-                c.w[4] = kFlagNonEmpty | kFlagOverflow;
+                x.e = kFlagNonEmpty | kFlagOverflow;
                 return true;
             }
-            I128 x = ld_d128(v, o.col, r);
-            c.w[0] = (uint32_t)x.lo;
-            c.w[1] = (uint32_t)(x.lo >> 32);
-            c.w[2] = (uint32_t)(uint64_t)x.hi;
-            c.w[3] = (uint64_t)(int64_t)(int32_t)(x.hi >> 32);
-            c.w[4] = kFlagNonEmpty;
+            I128 d = ld_d128(v, o.col, r);
+            x.a = d.lo;
+            x.b = (uint64_t)d.hi;
+            x.e = kFlagNonEmpty;
             return true;
         }
         case OP_MERGE_DAVG: {
             // WideDecimalAvgMergeAgg.merge (VectorAggregates.scala:557-573): counts add when valid;
             // a null sum poisons the group.
-            bool any = false;
-            if (col_valid(v, o.col2, r)) {
-                int64_t n = ld_i64(v, o.col2, r);
-                c.w[4] = (uint64_t)(uint32_t)n;
-                c.w[5] = (uint64_t)(int64_t)(int32_t)(n >> 32);
-                any = true;
-            }
+            if (col_valid(v, o.col2, r)) x.e = (uint64_t)ld_i64(v, o.col2, r);
             if (!col_valid(v, o.col, r)) {
-                c.w[6] = kFlagOverflow;
+                x.g = kFlagOverflow;
                 return true;
             }
-            I128 x = ld_d128(v, o.col, r);
-            c.w[0] = (uint32_t)x.lo;
-            c.w[1] = (uint32_t)(x.lo >> 32);
-            c.w[2] = (uint32_t)(uint64_t)x.hi;
-            c.w[3] = (uint64_t)(int64_t)(int32_t)(x.hi >> 32);
-            (void)any;
+            I128 d = ld_d128(v, o.col, r);
+            x.a = d.lo;
+            x.b = (uint64_t)d.hi;
             return true;
         }
     }
     return false;
 }
 
-// Kinds of an op's contribution words (mirrors the host's word_kind table).
-VR_DEV uint8_t op_word_kind(const Program& P, const OpDesc& o, int i) { return P.word_kind[o.word + i]; }
+// 128-bit value (lo, hi) as four 32-bit carry-save limbs (limb 3 signed).
+VR_DEV void limbs_of(uint64_t lo, uint64_t hi, uint64_t& l0, uint64_t& l1, uint64_t& l2, uint64_t& l3) {
+    l0 = (uint32_t)lo;
+    l1 = lo >> 32;
+    l2 = (uint32_t)hi;
+    l3 = hi32((int64_t)hi);
+}
+
+// raw -> global representation, in place.
+template <int K>
+VR_DEV void raw_to_global(const OpDesc& o, Contrib& x) {
+    (void)o;
+    switch (K) {
+        case OP_SUM_I64: {
+            int64_t v = (int64_t)x.a;
+            x.a = lo32(v);
+            x.b = hi32(v);
+            break;
+        }
+        case OP_SUM_D128:
+            limbs_of(x.a, x.b, x.a, x.b, x.c, x.d);
+            break;
+        case OP_SUM_PROD:
+            if (x.e) {
+                uint64_t lo = x.c, hi = x.d;
+                x.a = x.b = 0;
+                limbs_of(lo, hi, x.c, x.d, x.e, x.f);
+            } else {
+                int64_t v = (int64_t)x.a;
+                x.a = lo32(v);
+                x.b = hi32(v);
+            }
+            break;
+        case OP_MERGE_DSUM:
+            limbs_of(x.a, x.b, x.a, x.b, x.c, x.d);
+            break;
+        case OP_MERGE_DAVG: {
+            int64_t n = (int64_t)x.e;
+            limbs_of(x.a, x.b, x.a, x.b, x.c, x.d);
+            x.e = lo32(n);
+            x.f = hi32(n);
+            break;
+        }
+        default:
+            break;
+    }
+}
 
 // ------------------------------------------------- double-double add ----
 VR_DEV void two_sum(double a, double b, double& s, double& e) {
@@ -639,131 +812,14 @@ VR_DEV void dd_add(double& s, double& c, double s2, double c2) {
 VR_DEV bool u128_gt(uint64_t alo, uint64_t ahi, uint64_t blo, uint64_t bhi) {
     return ahi > bhi || (ahi == bhi && alo > blo);
 }
-
-// Combines contribution b into a (same op), word kind by word kind.
-VR_DEV void contrib_combine(const Program& P, const OpDesc& o, Contrib& a, const Contrib& b) {
-    for (int i = 0; i < o.nwords; ++i) {
-        switch (op_word_kind(P, o, i)) {
-            case WK_ADD: a.w[i] += b.w[i]; break;
-            case WK_MAX: a.w[i] = a.w[i] > b.w[i] ? a.w[i] : b.w[i]; break;
-            case WK_OR: a.w[i] |= b.w[i]; break;
-            case WK_F64: {
-                double s = __longlong_as_double((long long)a.w[i]), c = __longlong_as_double((long long)a.w[i + 1]);
-                dd_add(s, c, __longlong_as_double((long long)b.w[i]), __longlong_as_double((long long)b.w[i + 1]));
-                a.w[i] = (uint64_t)__double_as_longlong(s);
-                a.w[i + 1] = (uint64_t)__double_as_longlong(c);
-                ++i;
-                break;
-            }
-            case WK_MAX128:
-                if (u128_gt(b.w[i], b.w[i + 1], a.w[i], a.w[i + 1])) {
-                    a.w[i] = b.w[i];
-                    a.w[i + 1] = b.w[i + 1];
-                }
-                ++i;
-                break;
-            default: break;
-        }
-    }
-}
-
-// Applies a contribution to accumulator words `acc` (this op's first word)
-// with atomics in shared (S) or global memory. Zero words are skipped: every
-// word kind has identity 0.
-template <bool S>
-VR_DEV void contrib_apply(const Program& P, const OpDesc& o, uint64_t* acc, const Contrib& c) {
-    for (int i = 0; i < o.nwords; ++i) {
-        uint8_t kind = op_word_kind(P, o, i);
-        switch (kind) {
-            case WK_ADD:
-                if (c.w[i]) Mem<S>::add(acc + i, c.w[i]);
-                break;
-            case WK_MAX:
-                if (c.w[i]) Mem<S>::max(acc + i, c.w[i]);
-                break;
-            case WK_OR:
-                if (c.w[i]) Mem<S>::bor(acc + i, c.w[i]);
-                break;
-            case WK_F64: {
-                double s = __longlong_as_double((long long)c.w[i]);
-                double cc = __longlong_as_double((long long)c.w[i + 1]);
-                if (c.w[i] != 0 || c.w[i + 1] != 0) {
-                    // Compensated atomic: the hardware add rounds to nearest like __dadd_rn,
-                    // so the thread recovers the exact rounding error of its own add and
-                    // accumulates it (and the incoming compensation) in the next word.
-                    double old = Mem<S>::fadd(reinterpret_cast<double*>(acc + i), s);
-                    double nw, err;
-                    two_sum(old, s, nw, err);
-                    double tot = __dadd_rn(err, cc);
-                    if (tot != 0.0) Mem<S>::fadd(reinterpret_cast<double*>(acc + i + 1), tot);
-                }
-                ++i;
-                break;
-            }
-            case WK_MAX128: {
-                uint64_t lo = c.w[i], hi = c.w[i + 1];
-                if (lo | hi) {
-                    // 128-bit max by a 128-bit CAS loop (the pair is 16-byte aligned)
-                    uint64_t clo = Mem<S>::ld(acc + i), chi = Mem<S>::ld(acc + i + 1);
-                    for (int it = 0; it < 1 << 16 && u128_gt(lo, hi, clo, chi); ++it) {
-                        if (Mem<S>::cas128(acc + i, clo, chi, lo, hi)) break;
-                    }
-                }
-                ++i;
-                break;
-            }
-            default: break;
-        }
-    }
-}
-
-// Thread-private (non-atomic) apply for the direct tier: word i of the op
-// lives at acc[i * stride].
-VR_DEV void contrib_apply_private(const Program& P, const OpDesc& o, uint64_t* acc, int stride, const Contrib& c) {
-    for (int i = 0; i < o.nwords; ++i) {
-        uint8_t kind = op_word_kind(P, o, i);
-        uint64_t* p = acc + (int64_t)i * stride;
-        switch (kind) {
-            case WK_ADD:
-                if (c.w[i]) *p += c.w[i];
-                break;
-            case WK_MAX:
-                if (c.w[i] > *p) *p = c.w[i];
-                break;
-            case WK_OR:
-                *p |= c.w[i];
-                break;
-            case WK_F64: {
-                if (c.w[i] | c.w[i + 1]) {
-                    uint64_t* q = acc + (int64_t)(i + 1) * stride;
-                    double s = __longlong_as_double((long long)*p), cc = __longlong_as_double((long long)*q);
-                    dd_add(s, cc, __longlong_as_double((long long)c.w[i]), __longlong_as_double((long long)c.w[i + 1]));
-                    *p = (uint64_t)__double_as_longlong(s);
-                    *q = (uint64_t)__double_as_longlong(cc);
-                }
-                ++i;
-                break;
-            }
-            case WK_MAX128: {
-                uint64_t* q = acc + (int64_t)(i + 1) * stride;
-                if (u128_gt(c.w[i], c.w[i + 1], *p, *q)) {
-                    *p = c.w[i];
-                    *q = c.w[i + 1];
-                }
-                ++i;
-                break;
-            }
-            default: break;
-        }
-    }
-}
+VR_DEV double as_f64(uint64_t u) { return __longlong_as_double((long long)u); }
+VR_DEV uint64_t as_u64(double d) { return (uint64_t)__double_as_longlong(d); }
 
 // ------------------------------------------------ warp peer reduction ----
 // Peers are lanes holding the same key (from __match_any_sync). A tree over
-// each peer group's ranks: at step s, the lane of rank r (r % 2^(s+1) == 0)
-// takes the partial of rank r + 2^s. Rank -> lane uses nth_set_bit.
+// each peer group's ranks: at step s the lane of rank r (r % 2^(s+1) == 0)
+// takes the partial of rank r + 2^s. The lowest lane ends with the total.
 VR_DEV int nth_set_bit(uint32_t mask, int n) {
-    // position of the n-th (0-based) set bit of mask; mask has > n set bits
     int pos = 0;
 #pragma unroll
     for (int width = 16; width >= 1; width >>= 1) {
@@ -782,8 +838,8 @@ VR_DEV int nth_set_bit(uint32_t mask, int n) {
 
 struct PeerPlan {
     int steps;
-    int src[5];
-    uint32_t recv;  // bit s: this lane receives at step s
+    int src0, src1, src2, src3, src4;
+    uint32_t recv;  // bit s: this lane adds the partial it receives at step s
 };
 
 VR_DEV PeerPlan make_peer_plan(uint32_t peers, int lane) {
@@ -794,28 +850,426 @@ VR_DEV PeerPlan make_peer_plan(uint32_t peers, int lane) {
     pp.steps = 0;
     while ((1 << pp.steps) < maxn) ++pp.steps;
     pp.recv = 0;
+    int src[5];
 #pragma unroll
     for (int s = 0; s < 5; ++s) {
-        pp.src[s] = lane;
-        if (s < pp.steps) {
-            int stride = 1 << s;
-            if ((r % (2 * stride)) == 0 && r + stride < n) {
-                pp.recv |= 1u << s;
-                pp.src[s] = nth_set_bit(peers, r + stride);
-            }
+        src[s] = lane;
+        int stride = 1 << s;
+        if (s < pp.steps && (r % (2 * stride)) == 0 && r + stride < n) {
+            pp.recv |= 1u << s;
+            src[s] = nth_set_bit(peers, r + stride);
         }
     }
+    pp.src0 = src[0];
+    pp.src1 = src[1];
+    pp.src2 = src[2];
+    pp.src3 = src[3];
+    pp.src4 = src[4];
     return pp;
 }
 
-VR_DEV void peer_reduce(const Program& P, const OpDesc& o, const PeerPlan& pp, Contrib& c) {
-    for (int s = 0; s < pp.steps; ++s) {
-        Contrib t;
+VR_DEV int pp_src(const PeerPlan& pp, int s) {
+    return s == 0 ? pp.src0 : s == 1 ? pp.src1 : s == 2 ? pp.src2 : s == 3 ? pp.src3 : pp.src4;
+}
+
+enum RedKind { R_ADD, R_MAX, R_OR };
+
+template <int K>
+VR_DEV uint64_t red1(const PeerPlan& pp, uint64_t x) {
 #pragma unroll
-        for (int i = 0; i < kMaxContrib; ++i) {
-            t.w[i] = (i < o.nwords) ? (uint64_t)__shfl_sync(kFull, (unsigned long long)c.w[i], pp.src[s]) : 0;
+    for (int s = 0; s < 5; ++s) {
+        if (s < pp.steps) {
+            uint64_t t = (uint64_t)__shfl_sync(kFull, (unsigned long long)x, pp_src(pp, s));
+            if (pp.recv & (1u << s)) x = K == R_ADD ? x + t : K == R_MAX ? (t > x ? t : x) : (x | t);
         }
-        if (pp.recv & (1u << s)) contrib_combine(P, o, c, t);
+    }
+    return x;
+}
+
+VR_DEV void red_dd(const PeerPlan& pp, uint64_t& s_bits, uint64_t& c_bits) {
+#pragma unroll
+    for (int s = 0; s < 5; ++s) {
+        if (s < pp.steps) {
+            uint64_t ts = (uint64_t)__shfl_sync(kFull, (unsigned long long)s_bits, pp_src(pp, s));
+            uint64_t tc = (uint64_t)__shfl_sync(kFull, (unsigned long long)c_bits, pp_src(pp, s));
+            if (pp.recv & (1u << s)) {
+                double a = as_f64(s_bits), c = as_f64(c_bits);
+                dd_add(a, c, as_f64(ts), as_f64(tc));
+                s_bits = as_u64(a);
+                c_bits = as_u64(c);
+            }
+        }
+    }
+}
+
+VR_DEV void red_max128(const PeerPlan& pp, uint64_t& lo, uint64_t& hi) {
+#pragma unroll
+    for (int s = 0; s < 5; ++s) {
+        if (s < pp.steps) {
+            uint64_t tl = (uint64_t)__shfl_sync(kFull, (unsigned long long)lo, pp_src(pp, s));
+            uint64_t th = (uint64_t)__shfl_sync(kFull, (unsigned long long)hi, pp_src(pp, s));
+            if ((pp.recv & (1u << s)) && u128_gt(tl, th, lo, hi)) {
+                lo = tl;
+                hi = th;
+            }
+        }
+    }
+}
+
+// Combines the global-representation contribution over each peer group.
+template <int K>
+VR_DEV void peer_reduce(const OpDesc& o, const PeerPlan& pp, Contrib& x) {
+    (void)o;
+    switch (K) {
+        case OP_COUNT_ROWS:
+        case OP_COUNT_VALID:
+        case OP_SUM_I32:
+            x.a = red1<R_ADD>(pp, x.a);
+            break;
+        case OP_SUM_I64:
+            x.a = red1<R_ADD>(pp, x.a);
+            x.b = red1<R_ADD>(pp, x.b);
+            break;
+        case OP_SUM_F64:
+            red_dd(pp, x.a, x.b);
+            break;
+        case OP_SUM_D128:
+        case OP_MERGE_DSUM:
+        case OP_MERGE_DAVG:
+            x.a = red1<R_ADD>(pp, x.a);
+            x.b = red1<R_ADD>(pp, x.b);
+            x.c = red1<R_ADD>(pp, x.c);
+            x.d = red1<R_ADD>(pp, x.d);
+            if (K == OP_MERGE_DSUM) {
+                x.e = red1<R_OR>(pp, x.e);
+            } else if (K == OP_MERGE_DAVG) {
+                x.e = red1<R_ADD>(pp, x.e);
+                x.f = red1<R_ADD>(pp, x.f);
+                x.g = red1<R_OR>(pp, x.g);
+            }
+            break;
+        case OP_SUM_PROD: {
+            x.a = red1<R_ADD>(pp, x.a);
+            x.b = red1<R_ADD>(pp, x.b);
+            if (__any_sync(kFull, (x.c | x.d | x.e | x.f | x.g) != 0)) {  // rare: 128-bit products, errors
+                x.c = red1<R_ADD>(pp, x.c);
+                x.d = red1<R_ADD>(pp, x.d);
+                x.e = red1<R_ADD>(pp, x.e);
+                x.f = red1<R_ADD>(pp, x.f);
+                x.g = red1<R_OR>(pp, x.g);
+            }
+            x.h = red1<R_ADD>(pp, x.h);
+            break;
+        }
+        case OP_MAX_KEY:
+            x.a = red1<R_MAX>(pp, x.a);
+            break;
+        case OP_MAX_D128:
+            red_max128(pp, x.a, x.b);
+            break;
+    }
+}
+
+// ----------------------------------------------------- atomic apply ----
+template <bool S>
+VR_DEV void add_nz(uint64_t* p, uint64_t v) {
+    if (v) Mem<S>::add(p, v);
+}
+template <bool S>
+VR_DEV void or_nz(uint64_t* p, uint64_t v) {
+    if (v) Mem<S>::bor(p, v);
+}
+template <bool S>
+VR_DEV void max_nz(uint64_t* p, uint64_t v) {
+    if (v) Mem<S>::max(p, v);
+}
+// Compensated atomic add of a double-double (s, c): the hardware add rounds to
+// nearest like __dadd_rn, so the thread recovers the exact rounding error of
+// its own add and accumulates it (with the incoming compensation) in the next word.
+template <bool S>
+VR_DEV void fadd_pair(uint64_t* p, uint64_t s_bits, uint64_t c_bits) {
+    if (!(s_bits | c_bits)) return;
+    double s = as_f64(s_bits), cc = as_f64(c_bits);
+    double old = Mem<S>::fadd(reinterpret_cast<double*>(p), s);
+    double nw, err;
+    two_sum(old, s, nw, err);
+    double tot = __dadd_rn(err, cc);
+    if (tot != 0.0) Mem<S>::fadd(reinterpret_cast<double*>(p + 1), tot);
+}
+template <bool S>
+VR_DEV void max128(uint64_t* p, uint64_t lo, uint64_t hi) {
+    if (!(lo | hi)) return;
+    uint64_t clo = Mem<S>::ld(p), chi = Mem<S>::ld(p + 1);
+    for (int it = 0; it < (1 << 16) && u128_gt(lo, hi, clo, chi); ++it)
+        if (Mem<S>::cas128(p, clo, chi, lo, hi)) break;
+}
+
+// Applies a global-representation contribution to the op's words at `acc`.
+template <int K, bool S>
+VR_DEV void apply_global(const OpDesc& o, uint64_t* acc, const Contrib& x) {
+    (void)o;
+    switch (K) {
+        case OP_COUNT_ROWS:
+        case OP_COUNT_VALID:
+        case OP_SUM_I32:
+            add_nz<S>(acc, x.a);
+            break;
+        case OP_SUM_I64:
+            add_nz<S>(acc, x.a);
+            add_nz<S>(acc + 1, x.b);
+            break;
+        case OP_SUM_F64:
+            fadd_pair<S>(acc, x.a, x.b);
+            break;
+        case OP_SUM_D128:
+            add_nz<S>(acc, x.a);
+            add_nz<S>(acc + 1, x.b);
+            add_nz<S>(acc + 2, x.c);
+            add_nz<S>(acc + 3, x.d);
+            break;
+        case OP_SUM_PROD:
+            add_nz<S>(acc, x.a);
+            add_nz<S>(acc + 1, x.b);
+            add_nz<S>(acc + 2, x.c);
+            add_nz<S>(acc + 3, x.d);
+            add_nz<S>(acc + 4, x.e);
+            add_nz<S>(acc + 5, x.f);
+            or_nz<S>(acc + 6, x.g);
+            add_nz<S>(acc + 7, x.h);
+            break;
+        case OP_MAX_KEY:
+            max_nz<S>(acc, x.a);
+            break;
+        case OP_MAX_D128:
+            max128<S>(acc, x.a, x.b);
+            break;
+        case OP_MERGE_DSUM:
+            add_nz<S>(acc, x.a);
+            add_nz<S>(acc + 1, x.b);
+            add_nz<S>(acc + 2, x.c);
+            add_nz<S>(acc + 3, x.d);
+            or_nz<S>(acc + 4, x.e);
+            break;
+        case OP_MERGE_DAVG:
+            add_nz<S>(acc, x.a);
+            add_nz<S>(acc + 1, x.b);
+            add_nz<S>(acc + 2, x.c);
+            add_nz<S>(acc + 3, x.d);
+            add_nz<S>(acc + 4, x.e);
+            add_nz<S>(acc + 5, x.f);
+            or_nz<S>(acc + 6, x.g);
+            break;
+    }
+}
+
+// Compile-time op kinds: dispatch_kind(kind, f) calls f(KindTag<K>{}) with the
+// runtime kind as a constant, so per-kind code folds its switches away.
+template <int K>
+struct KindTag {
+    static constexpr int value = K;
+};
+template <class F>
+VR_DEV void dispatch_kind(int kind, F&& f) {
+    switch (kind) {
+        case OP_COUNT_ROWS: f(KindTag<OP_COUNT_ROWS>{}); break;
+        case OP_COUNT_VALID: f(KindTag<OP_COUNT_VALID>{}); break;
+        case OP_SUM_I32: f(KindTag<OP_SUM_I32>{}); break;
+        case OP_SUM_I64: f(KindTag<OP_SUM_I64>{}); break;
+        case OP_SUM_F64: f(KindTag<OP_SUM_F64>{}); break;
+        case OP_SUM_D128: f(KindTag<OP_SUM_D128>{}); break;
+        case OP_SUM_PROD: f(KindTag<OP_SUM_PROD>{}); break;
+        case OP_MAX_KEY: f(KindTag<OP_MAX_KEY>{}); break;
+        case OP_MAX_D128: f(KindTag<OP_MAX_D128>{}); break;
+        case OP_MERGE_DSUM: f(KindTag<OP_MERGE_DSUM>{}); break;
+        case OP_MERGE_DAVG: f(KindTag<OP_MERGE_DAVG>{}); break;
+    }
+}
+
+// Loads an op's global-representation state (a table slot's words) so it can
+// be applied to another table (shared-tier flush, rehash, spill merge).
+VR_DEV void load_state(const OpDesc& o, const uint64_t* acc, Contrib& x) {
+    czero(x);
+    int n = o.nwords;
+    x.a = acc[0];
+    if (n > 1) x.b = acc[1];
+    if (n > 2) x.c = acc[2];
+    if (n > 3) x.d = acc[3];
+    if (n > 4) x.e = acc[4];
+    if (n > 5) x.f = acc[5];
+    if (n > 6) x.g = acc[6];
+    if (n > 7) x.h = acc[7];
+}
+
+// ------------------------------------------------ thread-private apply ----
+// Direct tier: each consumer thread keeps an op's hot words (the running
+// values every row touches) privately, word i at hot[i * stride]; rare
+// events (64/128-bit wraps, 128-bit products, null products, error flags)
+// go with shared-memory atomics into a per-CTA copy of the op's global words
+// (`cold`). Hot words per kind: 1, except SUM_F64 / SUM_D128 / MAX_D128 (2:
+// sum+compensation, lo+hi) and MERGE_DSUM / MERGE_DAVG (3: lo, hi, flags or count).
+
+// hot += v; a signed wrap adds +-2^64 to the cold carry-save high word (+-2^32 there).
+VR_DEV void hot_add_i64(uint64_t* hot, uint64_t* cold_hi, int64_t v) {
+    int64_t s = (int64_t)*hot;
+    int64_t ns = (int64_t)((uint64_t)s + (uint64_t)v);
+    if (((s ^ ns) & (v ^ ns)) < 0) s_add(cold_hi, v > 0 ? (1ull << 32) : (0ull - (1ull << 32)));
+    *hot = (uint64_t)ns;
+}
+// (lo, hi) += (xlo, xhi) as int128; a wrap adds +-2^128 to the cold limb 3 (+-2^32 there).
+VR_DEV void hot_add_i128(uint64_t* lo, uint64_t* hi, uint64_t* cold_l3, uint64_t xlo, uint64_t xhi) {
+    uint64_t l = *lo, h = *hi;
+    uint64_t nl = l + xlo;
+    uint64_t nh = h + xhi + (nl < l ? 1 : 0);
+    if ((int64_t)((h ^ nh) & (xhi ^ nh)) < 0) s_add(cold_l3, (int64_t)xhi >= 0 ? (1ull << 32) : (0ull - (1ull << 32)));
+    *lo = nl;
+    *hi = nh;
+}
+
+template <int K>
+VR_DEV void apply_private(const OpDesc& o, uint64_t* hot, int stride, uint64_t* cold, const Contrib& x) {
+    (void)o;
+    switch (K) {
+        case OP_COUNT_ROWS:
+        case OP_COUNT_VALID:
+        case OP_SUM_I32:
+            hot[0] += x.a;
+            break;
+        case OP_SUM_I64:
+            hot_add_i64(hot, cold + 1, (int64_t)x.a);
+            break;
+        case OP_SUM_F64: {
+            double s = as_f64(hot[0]), c = as_f64(hot[stride]), v = as_f64(x.a);
+            double t = __dadd_rn(s, v);
+            if (isfinite(t))
+                c = __dadd_rn(c, fabs(s) >= fabs(v) ? __dadd_rn(__dsub_rn(s, t), v) : __dadd_rn(__dsub_rn(v, t), s));
+            hot[0] = as_u64(t);
+            hot[stride] = as_u64(c);
+            break;
+        }
+        case OP_SUM_D128:
+            hot_add_i128(hot, hot + stride, cold + 3, x.a, x.b);
+            break;
+        case OP_SUM_PROD:
+            if (x.h) {
+                s_add(cold + 7, 1);
+                if (x.g) s_or(cold + 6, 1);
+            } else if (x.e) {
+                uint64_t l0, l1, l2, l3;
+                limbs_of(x.c, x.d, l0, l1, l2, l3);
+                s_add(cold + 2, l0);
+                s_add(cold + 3, l1);
+                s_add(cold + 4, l2);
+                s_add(cold + 5, l3);
+            } else {
+                hot_add_i64(hot, cold + 1, (int64_t)x.a);
+            }
+            break;
+        case OP_MAX_KEY:
+            if (x.a > hot[0]) hot[0] = x.a;
+            break;
+        case OP_MAX_D128:
+            if (u128_gt(x.a, x.b, hot[0], hot[stride])) {
+                hot[0] = x.a;
+                hot[stride] = x.b;
+            }
+            break;
+        case OP_MERGE_DSUM:
+            hot[2 * stride] |= x.e;
+            if (x.a | x.b) hot_add_i128(hot, hot + stride, cold + 3, x.a, x.b);
+            break;
+        case OP_MERGE_DAVG:
+            if (x.e) hot_add_i64(hot + 2 * stride, cold + 5, (int64_t)x.e);
+            if (x.g) s_or(cold + 6, x.g);
+            if (x.a | x.b) hot_add_i128(hot, hot + stride, cold + 3, x.a, x.b);
+            break;
+    }
+}
+
+// ----------------------------------------------- private -> global flush ----
+// A signed 192-bit accumulator (lo: 128 bits, hi: the rest) for exact sums of
+// thread-private partials.
+struct Acc192 {
+    unsigned __int128 lo;
+    int64_t hi;
+};
+VR_DEV void acc_zero(Acc192& a) {
+    a.lo = 0;
+    a.hi = 0;
+}
+VR_DEV void acc_add_i128(Acc192& a, uint64_t xlo, uint64_t xhi) {
+    unsigned __int128 x = ((unsigned __int128)xhi << 64) | xlo;
+    unsigned __int128 n = a.lo + x;
+    a.hi += (n < a.lo ? 1 : 0) + ((int64_t)xhi < 0 ? -1 : 0);
+    a.lo = n;
+}
+VR_DEV void acc_add_i64(Acc192& a, int64_t v) { acc_add_i128(a, (uint64_t)v, v < 0 ? ~0ull : 0ull); }
+// Global carry-save words (lo32 unsigned, rest signed) that add the value.
+VR_DEV void acc_to_cs(const Acc192& a, uint64_t& w0, uint64_t& w1) {
+    w0 = (uint32_t)a.lo;
+    w1 = (uint64_t)(a.lo >> 32);  // exact while |value| < 2^95
+}
+VR_DEV void acc_to_limbs(const Acc192& a, uint64_t& l0, uint64_t& l1, uint64_t& l2, uint64_t& l3) {
+    l0 = (uint32_t)a.lo;
+    l1 = (uint32_t)(a.lo >> 32);
+    l2 = (uint32_t)(a.lo >> 64);
+    l3 = (uint64_t)(((int64_t)a.hi << 32) | (int64_t)(uint64_t)(a.lo >> 96));  // value >> 96, |value| < 2^159
+}
+
+// Combines the hot words of one op over all nt consumer threads (word i of
+// thread t at hot[i * nt + t]) into a global-representation contribution.
+template <int K>
+VR_DEV void private_to_global(const OpDesc& o, const uint64_t* hot, int nt, Contrib& x) {
+    (void)o;
+    czero(x);
+    const int64_t S = nt;
+    switch (K) {
+        case OP_COUNT_ROWS:
+        case OP_COUNT_VALID:
+        case OP_SUM_I32:
+            for (int t = 0; t < nt; ++t) x.a += hot[t];
+            break;
+        case OP_MAX_KEY:
+            for (int t = 0; t < nt; ++t) x.a = hot[t] > x.a ? hot[t] : x.a;
+            break;
+        case OP_MAX_D128:
+            for (int t = 0; t < nt; ++t)
+                if (u128_gt(hot[t], hot[S + t], x.a, x.b)) {
+                    x.a = hot[t];
+                    x.b = hot[S + t];
+                }
+            break;
+        case OP_SUM_F64: {
+            double s = 0.0, c = 0.0;
+            for (int t = 0; t < nt; ++t) dd_add(s, c, as_f64(hot[t]), as_f64(hot[S + t]));
+            x.a = as_u64(s);
+            x.b = as_u64(c);
+            break;
+        }
+        case OP_SUM_I64:
+        case OP_SUM_PROD: {
+            Acc192 a;
+            acc_zero(a);
+            for (int t = 0; t < nt; ++t) acc_add_i64(a, (int64_t)hot[t]);
+            acc_to_cs(a, x.a, x.b);
+            break;
+        }
+        case OP_SUM_D128:
+        case OP_MERGE_DSUM:
+        case OP_MERGE_DAVG: {
+            Acc192 a;
+            acc_zero(a);
+            for (int t = 0; t < nt; ++t) acc_add_i128(a, hot[t], hot[S + t]);
+            acc_to_limbs(a, x.a, x.b, x.c, x.d);
+            if (K == OP_MERGE_DSUM) {
+                for (int t = 0; t < nt; ++t) x.e |= hot[2 * S + t];
+            } else if (K == OP_MERGE_DAVG) {
+                Acc192 n;
+                acc_zero(n);
+                for (int t = 0; t < nt; ++t) acc_add_i64(n, (int64_t)hot[2 * S + t]);
+                acc_to_cs(n, x.e, x.f);
+            }
+            break;
+        }
     }
 }
 

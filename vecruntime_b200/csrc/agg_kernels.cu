@@ -25,460 +25,18 @@
 
 namespace vr {
 
-// --------------------------------------------------------------- smem map
-static __host__ __device__ inline int32_t align_up(int32_t x, int32_t a) { return (x + a - 1) / a * a; }
+}  // namespace vr
 
-struct StageHdr {
-    int64_t tile;  // -1: no more work
-    int64_t row0;
-    int32_t inst;
-    int32_t rows;
-    TileView view;
-};
+#include "agg_main.cuh"
 
-__host__ __device__ inline SmemMap smem_map_impl(int stages, int stage_bytes, int tier_bytes) {
-    SmemMap m;
-    m.prog = 0;
-    m.desc = align_up((int32_t)sizeof(Program), 16);
-    m.bars = align_up(m.desc + (int32_t)sizeof(BatchDesc), 16);
-    m.hdr = align_up(m.bars + 2 * kMaxStages * 8, 16);
-    m.stages = align_up(m.hdr + kMaxStages * (int32_t)sizeof(StageHdr), 128);
-    m.tier = align_up(m.stages + stages * stage_bytes, 128);
-    m.total = m.tier + tier_bytes;
-    return m;
-}
-SmemMap smem_map(int stages, int stage_bytes, int tier_bytes) { return smem_map_impl(stages, stage_bytes, tier_bytes); }
+namespace vr {
 
-VR_DEV void consumer_bar(int nt) { asm volatile("bar.sync 1, %0;" ::"r"(nt) : "memory"); }
-
-VR_DEV void set_error(uint64_t* ctrl, uint64_t bits) { atomicOr((unsigned long long*)&ctrl[CTRL_ERROR], bits); }
-
-// Copies n bytes (multiple of 8) global -> shared cooperatively.
-VR_DEV void coop_copy(void* dst, const void* src, int bytes, int tid, int nt) {
-    const uint64_t* s = reinterpret_cast<const uint64_t*>(src);
-    uint64_t* d = reinterpret_cast<uint64_t*>(dst);
-    for (int i = tid; i < bytes / 8; i += nt) d[i] = s[i];
-}
-
-// ------------------------------------------------------------ producer ---
-// Locates the instance owning global tile t (descs sorted by tile_begin).
-VR_DEV int find_instance(const BatchDesc* descs, int n, int64_t t) {
-    int lo = 0, hi = n - 1;
-    while (lo < hi) {
-        int mid = (lo + hi + 1) >> 1;
-        if (descs[mid].tile_begin <= t)
-            lo = mid;
-        else
-            hi = mid - 1;
-    }
-    return lo;
-}
-
-VR_DEV void producer_loop(const Program& P, const BatchDesc* __restrict__ descs, const LaunchCfg& cfg,
-                          uint64_t* tile_counter, uint64_t* full, uint64_t* empty, StageHdr* hdr,
-                          unsigned char* stage0) {
-    const int NS = cfg.stages;
-    const int T = cfg.tile_rows;
-    for (int64_t k = 0;; ++k) {
-        int s = (int)(k % NS);
-        uint32_t parity = (uint32_t)((k / NS) & 1);
-        if (!mbar_wait(&empty[s], parity ^ 1u)) {
-            set_error(descs[0].ctrl, kErrTimeout);
-            return;
-        }
-        int64_t t = (int64_t)atomicAdd((unsigned long long*)tile_counter, 1ull);
-        StageHdr& h = hdr[s];
-        if (t >= cfg.total_tiles) {
-            h.tile = -1;
-            mbar_arrive(&full[s]);
-            return;
-        }
-        int inst = cfg.num_desc == 1 ? 0 : find_instance(descs, cfg.num_desc, t);
-        const BatchDesc& d = descs[inst];
-        int64_t row0 = (t - d.tile_begin) * (int64_t)T;
-        int64_t left = d.num_rows - row0;
-        int rows = (int)(left < T ? left : T);
-        h.tile = t;
-        h.row0 = row0;
-        h.inst = inst;
-        h.rows = rows;
-        unsigned char* st = stage0 + (size_t)s * cfg.lay.stage_bytes;
-        bool bulk = d.tma && rows == T;
-        uint32_t bytes = 0;
-        for (int c = 0; c < P.num_cols; ++c) {
-            int w = P.col_width[c];
-            uint32_t db = w ? (uint32_t)(T * w) : (uint32_t)(T / 8);
-            const char* src = d.col_data[c] + (w ? row0 * w : row0 / 8);
-            h.view.data[c] = bulk ? (const char*)(st + cfg.lay.data_off[c]) : src;
-            bytes += bulk ? db : 0;
-            const uint32_t* vsrc = d.col_valid[c] ? d.col_valid[c] + row0 / 32 : nullptr;
-            if (vsrc && cfg.lay.valid_off[c] >= 0 && bulk) {
-                h.view.valid[c] = reinterpret_cast<const uint32_t*>(st + cfg.lay.valid_off[c]);
-                bytes += (uint32_t)(T / 8);
-            } else {
-                h.view.valid[c] = vsrc;
-            }
-        }
-        const uint32_t* ssrc = d.selection ? d.selection + row0 / 32 : nullptr;
-        if (ssrc && cfg.lay.sel_off >= 0 && bulk) {
-            h.view.sel = reinterpret_cast<const uint32_t*>(st + cfg.lay.sel_off);
-            bytes += (uint32_t)(T / 8);
-        } else {
-            h.view.sel = ssrc;
-        }
-        if (bulk) {
-            mbar_arrive_expect_tx(&full[s], bytes);
-            for (int c = 0; c < P.num_cols; ++c) {
-                int w = P.col_width[c];
-                uint32_t db = w ? (uint32_t)(T * w) : (uint32_t)(T / 8);
-                bulk_g2s(st + cfg.lay.data_off[c], d.col_data[c] + (w ? row0 * w : row0 / 8), db, &full[s]);
-                if (d.col_valid[c] && cfg.lay.valid_off[c] >= 0)
-                    bulk_g2s(st + cfg.lay.valid_off[c], d.col_valid[c] + row0 / 32, (uint32_t)(T / 8), &full[s]);
-            }
-            if (ssrc && cfg.lay.sel_off >= 0) bulk_g2s(st + cfg.lay.sel_off, ssrc, (uint32_t)(T / 8), &full[s]);
-        } else {
-            mbar_arrive(&full[s]);
-        }
-    }
-}
-
-// ------------------------------------------------------- row processing ---
-VR_DEV void defer_row(const BatchDesc& D, int64_t row) {
-    unsigned long long i = atomicAdd((unsigned long long*)&D.ctrl[CTRL_DEFERRED], 1ull);
-    if ((int64_t)i < D.deferred_cap)
-        D.deferred[i] = row;
-    else
-        set_error(D.ctrl, kErrDeferredFull);
-}
-
-// Hash tier: one warp-synchronous pass over up to 32 rows per warp. `r` is
-// the lane's row in view coordinates; `live` says whether it holds a row.
-template <int KW>
-VR_DEV void hash_rows_pass(const Program& P, const BatchDesc& D, const TileView& v, int64_t r, bool live,
-                           int64_t row_id, uint64_t* scache, int sslots, int s_probes, int g_probes,
-                           bool warp_agg, uint32_t& new_groups) {
-    const int lane = threadIdx.x & 31;
-    uint64_t key[KW];
-    bool side = false;
-    uint64_t h = 0;
-    if (live) {
-        bool bad;
-        pack_key<KW>(P, v, r, key, side, bad);
-        if (bad) {
-            set_error(D.ctrl, kErrBadKey);
-            live = false;
-        }
-        h = hash_key<KW>(key);
-    }
-    if (!live) {
-#pragma unroll
-        for (int i = 0; i < KW; ++i) key[i] = 0;
-    }
-    uint32_t peers = 1u << lane;
-    bool leader = live;
-    PeerPlan pp;
-    pp.steps = 0;
-    pp.recv = 0;
-    if (warp_agg) {
-        uint32_t livemask = __ballot_sync(kFull, live);
-        uint32_t m = kFull;
-#pragma unroll
-        for (int i = 0; i < KW; ++i) m &= __match_any_sync(kFull, (unsigned long long)key[i]);
-        m &= live ? livemask : ~livemask;
-        peers = m;
-        leader = live && ((__ffs(peers) - 1) == lane);
-        pp = make_peer_plan(peers, lane);
-    }
-    uint64_t* slot = nullptr;
-    bool in_smem = false, defer = false;
-    if (leader) {
-        bool fresh = false, to = false;
-        if (sslots > 0 && !side) {
-            slot = find_or_insert<true, KW>(scache, sslots - 1, P.sw, key, h >> 32, false, s_probes, fresh, to);
-            in_smem = slot != nullptr;
-        }
-        if (!slot) {
-            slot = find_or_insert<false, KW>(D.table, D.cap_mask, P.sw, key, h, side, g_probes, fresh, to);
-            if (slot && fresh) ++new_groups;
-            if (to) set_error(D.ctrl, kErrLockTimeout);
-            defer = (slot == nullptr) && !to;
-        }
-    }
-    if (warp_agg) {
-        uint32_t dm = __ballot_sync(kFull, defer);
-        if (dm) defer = live && ((dm >> (__ffs(peers) - 1)) & 1u);
-    }
-    if (defer) defer_row(D, row_id);
-    for (int i = 0; i < P.num_ops; ++i) {
-        const OpDesc& o = P.ops[i];
-        Contrib c;
-        if (live) {
-            op_contrib(o, v, r, c);
-        } else {
-#pragma unroll
-            for (int j = 0; j < kMaxContrib; ++j) c.w[j] = 0;
-        }
-        if (warp_agg) peer_reduce(P, o, pp, c);
-        if (slot) {
-            if (in_smem)
-                contrib_apply<true>(P, o, slot + P.kw + o.word, c);
-            else
-                contrib_apply<false>(P, o, slot + P.kw + o.word, c);
-        }
-    }
-}
-
-// Direct tier: thread-private accumulators, word (g, w) of consumer thread
-// t at priv[(g * aw + w) * nt + t].
-VR_DEV void direct_row(const Program& P, const BatchDesc& D, const TileView& v, int64_t r, uint64_t* priv, int nt,
-                       int ctid) {
-    int64_t g = direct_index(P, v, r);
-    if (g < 0 || g >= P.direct_slots) {
-        set_error(D.ctrl, kErrBadKey);
-        return;
-    }
-    uint64_t* base = priv + (size_t)g * P.aw * nt + ctid;
-    for (int i = 0; i < P.num_ops; ++i) {
-        const OpDesc& o = P.ops[i];
-        Contrib c;
-        if (op_contrib(o, v, r, c) || o.kind == OP_COUNT_ROWS)
-            contrib_apply_private(P, o, base + (size_t)o.word * nt, nt, c);
-    }
-}
-
-// Applies one combined word pair (kind at word w) to global memory.
-VR_DEV void word_apply_global(uint8_t kind, uint64_t* p, uint64_t a, uint64_t b) {
-    switch (kind) {
-        case WK_ADD:
-            if (a) g_add(p, a);
-            break;
-        case WK_MAX:
-            if (a) g_max(p, a);
-            break;
-        case WK_OR:
-            if (a) g_or(p, a);
-            break;
-        case WK_F64: {
-            if (a | b) {
-                double s = __longlong_as_double((long long)a), cc = __longlong_as_double((long long)b);
-                double old = g_fadd(reinterpret_cast<double*>(p), s);
-                double nw, err;
-                two_sum(old, s, nw, err);
-                double tot = __dadd_rn(err, cc);
-                if (tot != 0.0) g_fadd(reinterpret_cast<double*>(p + 1), tot);
-            }
-            break;
-        }
-        case WK_MAX128: {
-            if (a | b) {
-                uint64_t clo = ld_relaxed_g(p), chi = ld_relaxed_g(p + 1);
-                for (int it = 0; it < 1 << 16 && u128_gt(a, b, clo, chi); ++it)
-                    if (g_cas128(p, clo, chi, a, b)) break;
-            }
-            break;
-        }
-        default: break;
-    }
-}
-
-// Direct tier flush: each consumer thread combines whole (group, word)
-// columns of the private area and applies them to the dense HBM table.
-VR_DEV void flush_direct(const Program& P, const BatchDesc& D, uint64_t* priv, int nt, int ctid) {
-    const int64_t G = P.direct_slots;
-    const int aw = P.aw;
-    for (int64_t q = ctid; q < G * aw; q += nt) {
-        int64_t g = q / aw;
-        int w = (int)(q % aw);
-        uint8_t kind = P.word_kind[w];
-        if (kind == WK_F64C || kind == WK_MAX128L) continue;
-        const uint64_t* col = priv + (size_t)q * nt;
-        uint64_t a = 0, b = 0;
-        switch (kind) {
-            case WK_ADD:
-                for (int t = 0; t < nt; ++t) a += col[t];
-                break;
-            case WK_MAX:
-                for (int t = 0; t < nt; ++t) a = col[t] > a ? col[t] : a;
-                break;
-            case WK_OR:
-                for (int t = 0; t < nt; ++t) a |= col[t];
-                break;
-            case WK_F64: {
-                const uint64_t* col2 = col + nt;
-                double s = 0.0, c = 0.0;
-                for (int t = 0; t < nt; ++t)
-                    dd_add(s, c, __longlong_as_double((long long)col[t]), __longlong_as_double((long long)col2[t]));
-                a = (uint64_t)__double_as_longlong(s);
-                b = (uint64_t)__double_as_longlong(c);
-                break;
-            }
-            case WK_MAX128: {
-                const uint64_t* col2 = col + nt;
-                for (int t = 0; t < nt; ++t)
-                    if (u128_gt(col[t], col2[t], a, b)) {
-                        a = col[t];
-                        b = col2[t];
-                    }
-                break;
-            }
-        }
-        uint64_t* gslot = D.table + (size_t)g * P.sw;
-        word_apply_global(kind, gslot + P.kw + w, a, b);
-        if (w == 0 && a != 0) {  // COUNT_ROWS: the group exists, store its key (same bits from every CTA)
-            uint64_t kbuf[kMaxKW];
-            direct_key(P, g, kbuf);
-            for (int i = 0; i < P.kw; ++i) gslot[i] = kbuf[i];
-        }
-    }
-}
-
-// Is slot occupied? Every live group has COUNT_ROWS (word 0) >= 1.
-VR_DEV bool slot_used(const Program& P, const uint64_t* slot) { return slot[P.kw] != 0; }
-
-// Merges one slot state (key + accumulators) into the HBM table of D.
-// Returns false when the table had no room.
-template <int KW>
-VR_DEV bool merge_state(const Program& P, const BatchDesc& D, const uint64_t* src, uint32_t& new_groups,
-                        int g_probes) {
-    uint64_t key[KW];
-#pragma unroll
-    for (int i = 0; i < KW; ++i) key[i] = src[i];
-    bool side = (P.occ_word < 0) && key[0] == 0;  // sentinel layout: stored 0 == the sentinel key
-    bool fresh = false, to = false;
-    uint64_t* slot = find_or_insert<false, KW>(D.table, D.cap_mask, P.sw, key, hash_key<KW>(key), side, g_probes,
-                                               fresh, to);
-    if (to) set_error(D.ctrl, kErrLockTimeout);
-    if (!slot) return false;
-    if (fresh) ++new_groups;
-    for (int i = 0; i < P.num_ops; ++i) {
-        const OpDesc& o = P.ops[i];
-        Contrib c;
-#pragma unroll
-        for (int j = 0; j < kMaxContrib; ++j) c.w[j] = j < o.nwords ? src[KW + o.word + j] : 0;
-        contrib_apply<false>(P, o, slot + KW + o.word, c);
-    }
-    return true;
-}
-
-// Hash tier flush: every occupied shared slot into HBM; slots HBM cannot
-// take go to the spill list (merged by the host after the table grows).
-template <int KW>
-VR_DEV void flush_hash(const Program& P, const BatchDesc& D, uint64_t* scache, int sslots, int nt, int ctid,
-                       uint32_t& new_groups, int g_probes) {
-    for (int i = ctid; i < sslots; i += nt) {
-        const uint64_t* s = scache + (size_t)i * P.sw;
-        if (!slot_used(P, s)) continue;
-        if (!merge_state<KW>(P, D, s, new_groups, g_probes)) {
-            unsigned long long k = atomicAdd((unsigned long long*)&D.ctrl[CTRL_SPILLED], 1ull);
-            if ((int64_t)k < D.spill_cap) {
-                uint64_t* dst = D.spill + (size_t)k * P.sw;
-                for (int w = 0; w < P.sw; ++w) dst[w] = s[w];
-            } else {
-                set_error(D.ctrl, kErrSpillFull);
-            }
-        }
-    }
-}
-
-VR_DEV void zero_words(uint64_t* p, int64_t n, int tid, int nt) {
-    for (int64_t i = tid; i < n; i += nt) p[i] = 0;
-}
-
-// ---------------------------------------------------------- the kernel ---
 template <int KW, int TIER>
-__global__ void __launch_bounds__(kMaxConsumerThreads + 32) k_aggregate(const BatchDesc* __restrict__ descs,
+__global__ void __launch_bounds__(kMaxConsumerThreads + 32, 1) k_aggregate(const BatchDesc* __restrict__ descs,
                                                                         const LaunchCfg cfg,
                                                                         uint64_t* __restrict__ tile_counter) {
     extern __shared__ __align__(128) unsigned char smem[];
-    const SmemMap m = smem_map_impl(cfg.stages, cfg.lay.stage_bytes, cfg.tier_bytes);
-    Program& P = *reinterpret_cast<Program*>(smem + m.prog);
-    BatchDesc& D = *reinterpret_cast<BatchDesc*>(smem + m.desc);
-    uint64_t* full = reinterpret_cast<uint64_t*>(smem + m.bars);
-    uint64_t* empty = full + kMaxStages;
-    StageHdr* hdr = reinterpret_cast<StageHdr*>(smem + m.hdr);
-    unsigned char* stage0 = smem + m.stages;
-    uint64_t* tier = reinterpret_cast<uint64_t*>(smem + m.tier);
-
-    const int tid = threadIdx.x;
-    const int NT = cfg.consumer_threads;
-    coop_copy(&P, descs[0].prog, (int)sizeof(Program), tid, blockDim.x);
-    if (tid == 0) {
-        for (int s = 0; s < cfg.stages; ++s) {
-            mbar_init(&full[s], 1);
-            mbar_init(&empty[s], (uint32_t)(NT / 32));
-        }
-    }
-    __syncthreads();
-
-    if (tid >= NT) {  // producer warp
-        if (tid == NT) producer_loop(P, descs, cfg, tile_counter, full, empty, hdr, stage0);
-        return;
-    }
-
-    // consumer warps
-    const int ctid = tid;
-    const int sslots = cfg.tier_bytes / (8 * P.sw);
-    int cur = -1;
-    uint32_t new_groups = 0;
-    for (int64_t k = 0;; ++k) {
-        int s = (int)(k % cfg.stages);
-        uint32_t parity = (uint32_t)((k / cfg.stages) & 1);
-        if (!mbar_wait(&full[s], parity)) {
-            set_error(descs[0].ctrl, kErrTimeout);
-            break;
-        }
-        const StageHdr& h = hdr[s];
-        const int64_t tile = h.tile;
-        if (tile < 0) break;
-        const int inst = h.inst;
-        if (inst != cur) {  // uniform across consumer warps: they all see every tile
-            consumer_bar(NT);
-            if (cur >= 0) {
-                if (TIER == kTierDirect) {
-                    flush_direct(P, D, tier, NT, ctid);
-                } else {
-                    flush_hash<KW>(P, D, tier, D.smem_slots < sslots ? D.smem_slots : sslots, NT, ctid, new_groups,
-                                   cfg.g_probes);
-                }
-                if (new_groups) atomicAdd((unsigned long long*)&D.ctrl[CTRL_GROUPS], (unsigned long long)new_groups);
-                new_groups = 0;
-                consumer_bar(NT);
-            }
-            coop_copy(&D, &descs[inst], (int)sizeof(BatchDesc), ctid, NT);
-            zero_words(tier, cfg.tier_bytes / 8, ctid, NT);
-            consumer_bar(NT);
-            cur = inst;
-        }
-        const TileView& v = h.view;
-        const int rows = h.rows;
-        const int64_t row0 = h.row0;
-        if (TIER == kTierDirect) {
-            for (int r = ctid; r < rows; r += NT) {
-                if (v.sel && !bit_at(v.sel, r)) continue;
-                direct_row(P, D, v, r, tier, NT, ctid);
-            }
-        } else {
-            const int ss = D.smem_slots < sslots ? D.smem_slots : sslots;
-            const bool wa = D.warp_agg != 0;
-            for (int base = 0; base < rows; base += NT) {
-                int r = base + ctid;
-                bool live = r < rows && (v.sel == nullptr || bit_at(v.sel, r));
-                hash_rows_pass<KW>(P, D, v, r, live, row0 + r, tier, ss, cfg.s_probes, cfg.g_probes, wa, new_groups);
-            }
-        }
-        __syncwarp();
-        if ((ctid & 31) == 0) mbar_arrive(&empty[s]);
-    }
-    if (cur >= 0) {
-        consumer_bar(NT);
-        if (TIER == kTierDirect) {
-            flush_direct(P, D, tier, NT, ctid);
-        } else {
-            flush_hash<KW>(P, D, tier, D.smem_slots < sslots ? D.smem_slots : sslots, NT, ctid, new_groups,
-                           cfg.g_probes);
-        }
-        if (new_groups) atomicAdd((unsigned long long*)&D.ctrl[CTRL_GROUPS], (unsigned long long)new_groups);
-    }
+    aggregate_body<KW, TIER>(descs, cfg, tile_counter, smem);
 }
 
 // Deferred rows of one batch, against the HBM table only (rows are in batch
@@ -500,11 +58,11 @@ __global__ void k_replay(const BatchDesc* __restrict__ desc, const int64_t* __re
     uint32_t new_groups = 0;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     const int64_t first = (int64_t)blockIdx.x * blockDim.x;
-    for (int64_t base = first; base < n; base += stride) {  // warp-uniform trip count
+    for (int64_t base = first; base < n; base += stride) {
         int64_t i = base + threadIdx.x;
-        bool live = i < n;
-        int64_t r = live ? rows[i] : 0;
-        hash_rows_pass<KW>(P, D, v, r, live, r, nullptr, 0, 0, g_probes, false, new_groups);
+        bool live[1] = {i < n};
+        int64_t r[1] = {live[0] ? rows[i] : 0};
+        hash_chunk<KW, 1>(P, D, v, r, live, 0, nullptr, 0, 0, g_probes, false, new_groups);
     }
     if (new_groups) atomicAdd((unsigned long long*)&D.ctrl[CTRL_GROUPS], (unsigned long long)new_groups);
 }
@@ -631,7 +189,7 @@ VR_DEV OutVal out_value(const Program& P, const OutDesc& od, const uint64_t* slo
             break;
         }
         case OUT_COUNT:
-            r.lo = acc[od.w0];
+            r.lo = (od.flags & OUTF_NULLCOUNT) ? acc[0] - acc[od.w0] : acc[od.w0];
             break;
         case OUT_SUM_LONG:
         case OUT_SUM_LONG_NN: {
@@ -687,7 +245,7 @@ VR_DEV OutVal out_value(const Program& P, const OutDesc& od, const uint64_t* slo
         }
         case OUT_DEC_SUM: {
             // WideDecimalSumAgg / WideDecimalAvgAgg buffers (VectorAggregates.scala:329-347, 374-389, 466-477)
-            uint64_t cnt = acc[od.w1];
+            uint64_t cnt = (od.flags & OUTF_NULLCOUNT) ? acc[0] - acc[od.w1] : acc[od.w1];
             if (od.src_op == OP_SUM_PROD && (acc[od.w0 + 6] & 1)) emit_error(ctrl, VR_ERR_DECIMAL_PRECISION);
             bool of;
             Wide t = op_total(od.src_op, acc + od.w0, of);
@@ -710,7 +268,7 @@ VR_DEV OutVal out_value(const Program& P, const OutDesc& od, const uint64_t* slo
             if (od.flags & OUTF_FROM_FLAGS)
                 r.lo = (acc[od.w1] & kFlagNonEmpty) ? 0 : 1;
             else
-                r.lo = acc[od.w1] == 0 ? 1 : 0;
+                r.lo = ((od.flags & OUTF_NULLCOUNT) ? acc[0] - acc[od.w1] : acc[od.w1]) == 0 ? 1 : 0;
             break;
         case OUT_DEC_MERGE: {
             // WideDecimalSumMergeAgg.value / write (VectorAggregates.scala:727-766),
@@ -884,6 +442,27 @@ static cudaError_t launch_agg_t(const BatchDesc* descs, const LaunchCfg& cfg, in
     return cudaGetLastError();
 }
 
+template <int KW, int TIER>
+static int regs_t() {
+    cudaFuncAttributes a;
+    if (cudaFuncGetAttributes(&a, k_aggregate<KW, TIER>) != cudaSuccess) return 0;
+    return a.numRegs;
+}
+
+int aggregate_kernel_regs(int kw, int tier) {
+    switch (kw * 2 + (tier == kTierDirect ? 0 : 1)) {
+        case 2: return regs_t<1, kTierDirect>();
+        case 3: return regs_t<1, kTierHash>();
+        case 4: return regs_t<2, kTierDirect>();
+        case 5: return regs_t<2, kTierHash>();
+        case 6: return regs_t<3, kTierDirect>();
+        case 7: return regs_t<3, kTierHash>();
+        case 8: return regs_t<4, kTierDirect>();
+        case 9: return regs_t<4, kTierHash>();
+    }
+    return 0;
+}
+
 cudaError_t launch_aggregate(int kw, int tier, const BatchDesc* descs, const LaunchCfg& cfg, int blocks,
                              uint64_t* tile_counter, cudaStream_t stream) {
     if (tier == kTierDirect) {
@@ -962,19 +541,6 @@ cudaError_t launch_hash_rows(int num_keys, const vr_column_type* types_dev, cons
     if (n <= 0) return cudaSuccess;
     k_hash_rows<<<grid_for(n, 256), 256, 0, stream>>>(num_keys, types_dev, keys_dev, n, out, finish);
     return cudaGetLastError();
-}
-
-cudaError_t upload_pow10() {
-    uint64_t lo[39], hi[39];
-    unsigned __int128 v = 1;
-    for (int i = 0; i < 39; ++i) {
-        lo[i] = (uint64_t)v;
-        hi[i] = (uint64_t)(v >> 64);
-        v *= 10;
-    }
-    cudaError_t e = cudaMemcpyToSymbol(c_pow10_lo, lo, sizeof(lo));
-    if (e != cudaSuccess) return e;
-    return cudaMemcpyToSymbol(c_pow10_hi, hi, sizeof(hi));
 }
 
 }  // namespace vr

@@ -4,43 +4,17 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#include "vr_internal.h"
+#include "agg_types.h"
 
 namespace vr {
 
-// Where each staged column lands inside one pipeline stage.
-struct StageLayout {
-    int32_t data_off[kMaxCols];
-    int32_t valid_off[kMaxCols];  // -1: the column is never nullable
-    int32_t sel_off;              // -1: launches without selection bitmaps
-    int32_t stage_bytes;
-};
-
-struct LaunchCfg {
-    int32_t tile_rows;         // rows per tile, a multiple of 128
-    int32_t stages;            // pipeline depth
-    int32_t consumer_threads;  // multiple of 32; one extra producer warp follows
-    int32_t num_desc;          // instances in this launch
-    int64_t total_tiles;
-    int32_t g_probes;          // HBM table probe limit before a row is deferred
-    int32_t s_probes;          // shared-memory cache probe limit
-    int32_t smem_bytes;        // dynamic shared memory of the launch
-    int32_t tier_bytes;        // shared memory of the tier area
-    StageLayout lay;
-};
-
-// Shared-memory map of the aggregate kernel (same formula on host and device).
-struct SmemMap {
-    int32_t prog, desc, bars, hdr, stages, tier, total;
-};
 SmemMap smem_map(int stages, int stage_bytes, int tier_bytes);
-
-constexpr int kMaxStages = 4;
-constexpr int kMaxConsumerThreads = 512;
 
 // Launchers (all asynchronous on `stream`). `descs` lives in device memory.
 cudaError_t launch_aggregate(int kw, int tier, const BatchDesc* descs, const LaunchCfg& cfg, int blocks,
                              uint64_t* tile_counter, cudaStream_t stream);
+// Registers per thread of the ahead-of-time aggregate kernel (occupancy).
+int aggregate_kernel_regs(int kw, int tier);
 // Replays deferred rows of one batch against the HBM table (no shared tier).
 cudaError_t launch_replay(int kw, const BatchDesc* desc, const int64_t* rows, int64_t n, int g_probes,
                           cudaStream_t stream);
@@ -53,7 +27,6 @@ cudaError_t launch_merge_slots(int kw, const BatchDesc* desc, const uint64_t* sl
 cudaError_t launch_compact_kw(int kw, const uint64_t* table, int64_t slots, int sw, int64_t* out, int64_t* num_dev,
                               void* temp, size_t* temp_bytes, cudaStream_t stream);
 // Uploads the 10^p table used by the decimal precision checks (per device).
-cudaError_t upload_pow10();
 // Writes output rows [from, to) of the compacted groups into device columns.
 cudaError_t launch_emit(const Program* prog_dev, const EmitProgram* emit_dev, const uint64_t* table,
                         const int64_t* slot_of, int64_t from, int64_t to, const vr_out_column* outs_dev,

@@ -1,0 +1,537 @@
+// The aggregate kernel body and its helpers (device code only). Included by
+// the ahead-of-time kernels (agg_kernels.cu) and by the per-spec kernels
+// compiled at run time with NVRTC (jit.cpp), where VR_JIT is defined and the
+// Program is a compile-time constant: every loop over ops and key fields then
+// unrolls into straight-line code for that spec.
+#pragma once
+#include "agg_device.cuh"
+#include "agg_types.h"
+
+namespace vr {
+
+// --------------------------------------------------------------- smem map
+static __host__ __device__ inline int32_t align_up(int32_t x, int32_t a) { return (x + a - 1) / a * a; }
+
+struct StageHdr {
+    int64_t tile;  // -1: no more work
+    int64_t row0;
+    int32_t inst;
+    int32_t rows;
+    TileView view;
+};
+
+__host__ __device__ inline SmemMap smem_map_impl(int stages, int stage_bytes, int tier_bytes) {
+    SmemMap m;
+    m.prog = 0;
+    m.desc = align_up((int32_t)sizeof(Program), 16);
+    m.pdesc = align_up(m.desc + (int32_t)sizeof(BatchDesc), 16);  // the producer's own copy
+    m.bars = align_up(m.pdesc + (int32_t)sizeof(BatchDesc), 16);
+    m.hdr = align_up(m.bars + 2 * kMaxStages * 8, 16);
+    m.stages = align_up(m.hdr + kMaxStages * (int32_t)sizeof(StageHdr), 128);
+    m.tier = align_up(m.stages + stages * stage_bytes, 128);
+    m.total = m.tier + tier_bytes;
+    return m;
+}
+SmemMap smem_map(int stages, int stage_bytes, int tier_bytes) { return smem_map_impl(stages, stage_bytes, tier_bytes); }
+
+VR_DEV void consumer_bar(int nt) { asm volatile("bar.sync 1, %0;" ::"r"(nt) : "memory"); }
+
+VR_DEV void set_error(uint64_t* ctrl, uint64_t bits) { atomicOr((unsigned long long*)&ctrl[CTRL_ERROR], bits); }
+
+// Copies n bytes (multiple of 8) global -> shared cooperatively.
+VR_DEV void coop_copy(void* dst, const void* src, int bytes, int tid, int nt) {
+    const uint64_t* s = reinterpret_cast<const uint64_t*>(src);
+    uint64_t* d = reinterpret_cast<uint64_t*>(dst);
+    for (int i = tid; i < bytes / 8; i += nt) d[i] = s[i];
+}
+
+// ------------------------------------------------------------ producer ---
+// Locates the instance owning global tile t (descs sorted by tile_begin).
+VR_DEV int find_instance(const BatchDesc* descs, int n, int64_t t) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (descs[mid].tile_begin <= t)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+// The producer thread: fetches tile indices (one ahead, so the atomic's round
+// trip overlaps the previous tile's issue), finds the tile's instance with a
+// cursor that only moves forward (a producer's tile indices only grow), keeps
+// that instance's descriptor in its own shared-memory copy (reloaded only
+// when the instance changes), and issues the tile's bulk copies.
+VR_DEV void producer_loop(const Program& P, const BatchDesc* __restrict__ descs, const LaunchCfg& cfg,
+                          uint64_t* tile_counter, uint64_t* full, uint64_t* empty, StageHdr* hdr,
+                          unsigned char* stage0, BatchDesc* pd) {
+    const int NS = cfg.stages;
+    const int T = cfg.tile_rows;
+    int cur = -1;
+    int64_t t_next = (int64_t)atomicAdd((unsigned long long*)tile_counter, 1ull);
+    for (int64_t k = 0;; ++k) {
+        int s = (int)(k % NS);
+        uint32_t parity = (uint32_t)((k / NS) & 1);
+        if (!mbar_wait(&empty[s], parity ^ 1u)) {
+            set_error(descs[0].ctrl, kErrTimeout);
+            return;
+        }
+        const int64_t t = t_next;
+        StageHdr& h = hdr[s];
+        if (t >= cfg.total_tiles) {
+            h.tile = -1;
+            mbar_arrive(&full[s]);
+            return;
+        }
+        t_next = (int64_t)atomicAdd((unsigned long long*)tile_counter, 1ull);
+        int inst = cur < 0 ? 0 : cur;
+        if (cfg.num_desc > 1)
+            while (inst + 1 < cfg.num_desc && descs[inst + 1].tile_begin <= t) ++inst;
+        if (inst != cur) {
+            const uint64_t* src = reinterpret_cast<const uint64_t*>(&descs[inst]);
+            uint64_t* dst = reinterpret_cast<uint64_t*>(pd);
+            for (int i = 0; i < (int)(sizeof(BatchDesc) / 8); ++i) dst[i] = src[i];
+            cur = inst;
+        }
+        const BatchDesc& d = *pd;
+        int64_t row0 = (t - d.tile_begin) * (int64_t)T;
+        int64_t left = d.num_rows - row0;
+        int rows = (int)(left < T ? left : T);
+        h.tile = t;
+        h.row0 = row0;
+        h.inst = inst;
+        h.rows = rows;
+        unsigned char* st = stage0 + (size_t)s * cfg.lay.stage_bytes;
+        bool bulk = d.tma && rows == T;
+        uint32_t bytes = 0;
+        for (int c = 0; c < P.num_cols; ++c) {
+            int w = P.col_width[c];
+            uint32_t db = w ? (uint32_t)(T * w) : (uint32_t)(T / 8);
+            const char* src = d.col_data[c] + (w ? row0 * w : row0 / 8);
+            h.view.data[c] = bulk ? (const char*)(st + cfg.lay.data_off[c]) : src;
+            bytes += bulk ? db : 0;
+            const uint32_t* vsrc = d.col_valid[c] ? d.col_valid[c] + row0 / 32 : nullptr;
+            if (vsrc && cfg.lay.valid_off[c] >= 0 && bulk) {
+                h.view.valid[c] = reinterpret_cast<const uint32_t*>(st + cfg.lay.valid_off[c]);
+                bytes += (uint32_t)(T / 8);
+            } else {
+                h.view.valid[c] = vsrc;
+            }
+        }
+        const uint32_t* ssrc = d.selection ? d.selection + row0 / 32 : nullptr;
+        if (ssrc && cfg.lay.sel_off >= 0 && bulk) {
+            h.view.sel = reinterpret_cast<const uint32_t*>(st + cfg.lay.sel_off);
+            bytes += (uint32_t)(T / 8);
+        } else {
+            h.view.sel = ssrc;
+        }
+        if (bulk) {
+            mbar_arrive_expect_tx(&full[s], bytes);
+            for (int c = 0; c < P.num_cols; ++c) {
+                int w = P.col_width[c];
+                uint32_t db = w ? (uint32_t)(T * w) : (uint32_t)(T / 8);
+                bulk_g2s(st + cfg.lay.data_off[c], d.col_data[c] + (w ? row0 * w : row0 / 8), db, &full[s]);
+                if (d.col_valid[c] && cfg.lay.valid_off[c] >= 0)
+                    bulk_g2s(st + cfg.lay.valid_off[c], d.col_valid[c] + row0 / 32, (uint32_t)(T / 8), &full[s]);
+            }
+            if (ssrc && cfg.lay.sel_off >= 0) bulk_g2s(st + cfg.lay.sel_off, ssrc, (uint32_t)(T / 8), &full[s]);
+        } else {
+            mbar_arrive(&full[s]);
+        }
+    }
+}
+
+// ------------------------------------------------------- row processing ---
+VR_DEV void defer_row(const BatchDesc& D, int64_t row) {
+    unsigned long long i = atomicAdd((unsigned long long*)&D.ctrl[CTRL_DEFERRED], 1ull);
+    if ((int64_t)i < D.deferred_cap)
+        D.deferred[i] = row;
+    else
+        set_error(D.ctrl, kErrDeferredFull);
+}
+
+// One op over a hash-tier chunk: raw row values -> global representation ->
+// (optional) combine over key peers in the warp -> atomics on the row's slot
+// (shared cache or HBM). Kind K is a compile-time constant.
+template <int K, int R>
+VR_DEV void hash_op(const OpDesc& op, const TileView& v, const int64_t (&r)[R], const bool (&live)[R],
+                    uint64_t* const (&slot)[R], const bool (&in_smem)[R], const PeerPlan (&pp)[R], bool warp_agg) {
+    OpDesc o;
+    OpView ov;
+    make_opview(op, v, o, ov);
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+        Contrib c;
+        if (live[j])
+            op_raw<K>(o, ov, r[j], c);
+        else
+            czero(c);
+        raw_to_global<K>(o, c);
+        if (warp_agg) peer_reduce<K>(o, pp[j], c);
+        if (slot[j]) {
+            if (in_smem[j])
+                apply_global<K, true>(o, slot[j] + o.word, c);
+            else
+                apply_global<K, false>(o, slot[j] + o.word, c);
+        }
+    }
+}
+
+// One op over a direct-tier chunk: thread-private hot words, CTA cold words.
+template <int K, int R>
+VR_DEV void direct_op(const OpDesc& op, const TileView& v, const int64_t (&r)[R], const bool (&live)[R],
+                      const int (&g)[R], uint64_t* priv, uint64_t* cold, int nt, int ctid, int hw, int aw) {
+    OpDesc o;
+    OpView ov;
+    make_opview(op, v, o, ov);
+    uint64_t* hot = priv + (size_t)o.hword * nt + ctid;
+    uint64_t* cop = cold + o.word;
+    const size_t gstride = (size_t)hw * nt;
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+        Contrib c;
+        if (live[j] && op_raw<K>(o, ov, r[j], c))
+            apply_private<K>(o, hot + g[j] * gstride, nt, cop + (size_t)g[j] * aw, c);
+    }
+}
+
+#ifdef VR_JIT
+// Defined by the per-spec source after this header: jit_for_op(i, f) calls
+// f(op, KindTag<kind>{}) with op i's descriptor as a compile-time constant;
+// the key fields likewise. VR_JIT_NUM_OPS is the spec's op count.
+template <class F>
+VR_DEV void jit_for_op(int i, F&& f);
+VR_DEV int64_t jit_direct_index(const TileView& v, int64_t r);
+template <int KW>
+VR_DEV void jit_pack_key(const TileView& v, int64_t r, uint64_t (&k)[KW], bool& side, bool& bad);
+#define VR_NUM_OPS(P) VR_JIT_NUM_OPS
+#else
+#define VR_NUM_OPS(P) ((P).num_ops)
+#endif
+
+// f(op, KindTag<op kind>{}) for op i: the per-spec constant descriptor under
+// VR_JIT, else the program's descriptor with its kind dispatched at run time.
+template <class F>
+VR_DEV void for_op(const Program& P, int i, F&& f) {
+#ifdef VR_JIT
+    (void)P;
+    jit_for_op(i, f);
+#else
+    const OpDesc& op = P.ops[i];
+    dispatch_kind(op.kind, [&](auto tag) { f(op, tag); });
+#endif
+}
+
+// Hash tier: a chunk of R rows per consumer thread (row r[j]; warps stay
+// converged: every lane runs every j). Each row's key is resolved to a slot
+// (shared cache first, then HBM, else deferred); then every op runs once over
+// the chunk with its kind fixed at compile time, so the per-row work is
+// straight-line code.
+template <int KW, int R>
+VR_DEV void hash_chunk(const Program& P, const BatchDesc& D, const TileView& v, const int64_t (&r)[R],
+                       const bool (&live_in)[R], int64_t row_base, uint64_t* scache, int sslots, int s_probes,
+                       int g_probes, bool warp_agg, uint32_t& new_groups) {
+    const int lane = threadIdx.x & 31;
+    bool live[R];
+    uint64_t* slot[R];
+    bool in_smem[R];
+    PeerPlan pp[R];
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+        live[j] = live_in[j];
+        uint64_t key[KW];
+        bool side = false;
+        uint64_t h = 0;
+        if (live[j]) {
+            bool bad;
+#ifdef VR_JIT
+            jit_pack_key<KW>(v, r[j], key, side, bad);
+#else
+            pack_key<KW>(P, v, r[j], key, side, bad);
+#endif
+            if (bad) {
+                set_error(D.ctrl, kErrBadKey);
+                live[j] = false;
+            }
+            h = hash_key<KW>(key);
+        }
+        if (!live[j]) {
+#pragma unroll
+            for (int i = 0; i < KW; ++i) key[i] = 0;
+        }
+        uint32_t peers = 1u << lane;
+        bool leader = live[j];
+        pp[j].steps = 0;
+        pp[j].recv = 0;
+        if (warp_agg) {
+            uint32_t livemask = __ballot_sync(kFull, live[j]);
+            uint32_t m = kFull;
+#pragma unroll
+            for (int i = 0; i < KW; ++i) m &= __match_any_sync(kFull, (unsigned long long)key[i]);
+            m &= live[j] ? livemask : ~livemask;
+            peers = m;
+            leader = live[j] && ((__ffs(peers) - 1) == lane);
+            pp[j] = make_peer_plan(peers, lane);
+        }
+        slot[j] = nullptr;
+        in_smem[j] = false;
+        bool defer = false;
+        if (leader) {
+            bool fresh = false, to = false;
+            if (sslots > 0 && !side) {
+                slot[j] = find_or_insert<true, KW>(scache, sslots - 1, P.sw, key, h >> 32, false, s_probes, fresh, to);
+                in_smem[j] = slot[j] != nullptr;
+            }
+            if (!slot[j]) {
+                slot[j] = find_or_insert<false, KW>(D.table, D.cap_mask, P.sw, key, h, side, g_probes, fresh, to);
+                if (slot[j] && fresh) ++new_groups;
+                if (to) set_error(D.ctrl, kErrLockTimeout);
+                defer = (slot[j] == nullptr) && !to;
+            }
+        }
+        if (warp_agg) {
+            uint32_t dm = __ballot_sync(kFull, defer);
+            if (dm) defer = live[j] && ((dm >> (__ffs(peers) - 1)) & 1u);
+        }
+        if (defer) defer_row(D, row_base + r[j]);
+        if (slot[j]) slot[j] += P.kw;  // accumulator words
+    }
+    VR_UNROLL
+    for (int i = 0; i < VR_NUM_OPS(P); ++i)
+        for_op(P, i, [&](const OpDesc& op, auto tag) {
+            hash_op<decltype(tag)::value, R>(op, v, r, live, slot, in_smem, pp, warp_agg);
+        });
+}
+
+// Direct tier: hot word h of group g of consumer thread t at
+// priv[(g * hw + h) * nt + t]; the CTA's cold words of group g at
+// cold[g * aw + word]. A chunk of R rows per thread, every op once per chunk
+// (kind fixed at compile time, column pointers in registers).
+template <int R>
+VR_DEV void direct_chunk(const Program& P, const BatchDesc& D, const TileView& v, const int64_t (&r)[R],
+                         const bool (&live_in)[R], uint64_t* priv, uint64_t* cold, int nt, int ctid) {
+    bool live[R];
+    int g[R];
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+        live[j] = live_in[j];
+        g[j] = 0;
+        if (live[j]) {
+#ifdef VR_JIT
+            int64_t gi = jit_direct_index(v, r[j]);
+#else
+            int64_t gi = direct_index(P, v, r[j]);
+#endif
+            if (gi < 0 || gi >= P.direct_slots) {
+                set_error(D.ctrl, kErrBadKey);
+                live[j] = false;
+            } else {
+                g[j] = (int)gi;
+            }
+        }
+    }
+    const int hw = P.hw, aw = P.aw;
+    VR_UNROLL
+    for (int i = 0; i < VR_NUM_OPS(P); ++i)
+        for_op(P, i, [&](const OpDesc& op, auto tag) {
+            direct_op<decltype(tag)::value, R>(op, v, r, live, g, priv, cold, nt, ctid, hw, aw);
+        });
+}
+
+// Direct tier flush: each consumer thread takes whole (group, op) pairs,
+// combines the op's hot words over all consumer threads, adds the CTA's cold
+// words, and applies both to the dense HBM table with atomics.
+VR_DEV void flush_direct(const Program& P, const BatchDesc& D, uint64_t* priv, uint64_t* cold, int nt, int ctid) {
+    const int64_t G = P.direct_slots;
+    const int nops = P.num_ops;
+    for (int64_t q = ctid; q < G * nops; q += nt) {
+        int64_t g = q / nops;
+        uint64_t* gslot = D.table + (size_t)g * P.sw;
+        Contrib c;
+        bool rows_op = false;
+        for_op(P, (int)(q % nops), [&](const OpDesc& o, auto tag) {
+            constexpr int K = decltype(tag)::value;
+            private_to_global<K>(o, priv + ((size_t)g * P.hw + o.hword) * nt, nt, c);
+            apply_global<K, false>(o, gslot + P.kw + o.word, c);
+            Contrib cc;
+            load_state(o, cold + (size_t)g * P.aw + o.word, cc);
+            apply_global<K, false>(o, gslot + P.kw + o.word, cc);
+            rows_op = K == OP_COUNT_ROWS;
+        });
+        if (rows_op && c.a != 0) {  // the group exists: store its key (same bits from every CTA)
+            uint64_t kbuf[kMaxKW];
+            direct_key(P, g, kbuf);
+            for (int i = 0; i < P.kw; ++i) gslot[i] = kbuf[i];
+        }
+    }
+}
+
+// Is slot occupied? Every live group has COUNT_ROWS (word 0) >= 1.
+VR_DEV bool slot_used(const Program& P, const uint64_t* slot) { return slot[P.kw] != 0; }
+
+// Merges one slot state (key + accumulators) into the HBM table of D.
+// Returns false when the table had no room.
+template <int KW>
+VR_DEV bool merge_state(const Program& P, const BatchDesc& D, const uint64_t* src, uint32_t& new_groups,
+                        int g_probes) {
+    uint64_t key[KW];
+#pragma unroll
+    for (int i = 0; i < KW; ++i) key[i] = src[i];
+    bool side = (P.occ_word < 0) && key[0] == 0;  // sentinel layout: stored 0 == the sentinel key
+    bool fresh = false, to = false;
+    uint64_t* slot = find_or_insert<false, KW>(D.table, D.cap_mask, P.sw, key, hash_key<KW>(key), side, g_probes,
+                                               fresh, to);
+    if (to) set_error(D.ctrl, kErrLockTimeout);
+    if (!slot) return false;
+    if (fresh) ++new_groups;
+    VR_UNROLL
+    for (int i = 0; i < VR_NUM_OPS(P); ++i)
+        for_op(P, i, [&](const OpDesc& o, auto tag) {
+            Contrib c;
+            load_state(o, src + KW + o.word, c);
+            apply_global<decltype(tag)::value, false>(o, slot + KW + o.word, c);
+        });
+    return true;
+}
+
+// Hash tier flush: every occupied shared slot into HBM; slots HBM cannot
+// take go to the spill list (merged by the host after the table grows).
+template <int KW>
+VR_DEV void flush_hash(const Program& P, const BatchDesc& D, uint64_t* scache, int sslots, int nt, int ctid,
+                       uint32_t& new_groups, int g_probes) {
+    for (int i = ctid; i < sslots; i += nt) {
+        const uint64_t* s = scache + (size_t)i * P.sw;
+        if (!slot_used(P, s)) continue;
+        if (!merge_state<KW>(P, D, s, new_groups, g_probes)) {
+            unsigned long long k = atomicAdd((unsigned long long*)&D.ctrl[CTRL_SPILLED], 1ull);
+            if ((int64_t)k < D.spill_cap) {
+                uint64_t* dst = D.spill + (size_t)k * P.sw;
+                for (int w = 0; w < P.sw; ++w) dst[w] = s[w];
+            } else {
+                set_error(D.ctrl, kErrSpillFull);
+            }
+        }
+    }
+}
+
+VR_DEV void zero_words(uint64_t* p, int64_t n, int tid, int nt) {
+    for (int64_t i = tid; i < n; i += nt) p[i] = 0;
+}
+
+// ---------------------------------------------------------- the kernel ---
+// The kernel body; the ahead-of-time kernel (agg_kernels.cu) and the per-spec
+// kernels compiled at run time (jit.cpp) both wrap it.
+template <int KW, int TIER>
+VR_DEV void aggregate_body(const BatchDesc* __restrict__ descs, const LaunchCfg& cfg, uint64_t* __restrict__ tile_counter,
+                           unsigned char* smem) {
+    const SmemMap m = smem_map_impl(cfg.stages, cfg.lay.stage_bytes, cfg.tier_bytes);
+    const Program& P = VR_PROG(smem + m.prog);
+    BatchDesc& D = *reinterpret_cast<BatchDesc*>(smem + m.desc);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + m.bars);
+    uint64_t* empty = full + kMaxStages;
+    StageHdr* hdr = reinterpret_cast<StageHdr*>(smem + m.hdr);
+    unsigned char* stage0 = smem + m.stages;
+    uint64_t* tier = reinterpret_cast<uint64_t*>(smem + m.tier);
+
+    const int tid = threadIdx.x;
+    const int NT = cfg.consumer_threads;
+#ifndef VR_JIT
+    coop_copy(smem + m.prog, descs[0].prog, (int)sizeof(Program), tid, blockDim.x);
+#endif
+    if (tid == 0) {
+        for (int s = 0; s < cfg.stages; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], (uint32_t)(NT / 32));
+        }
+    }
+    __syncthreads();
+
+    if (tid >= NT) {  // producer warp
+        if (tid == NT)
+            producer_loop(P, descs, cfg, tile_counter, full, empty, hdr, stage0,
+                          reinterpret_cast<BatchDesc*>(smem + m.pdesc));
+        return;
+    }
+
+    // consumer warps
+    const int ctid = tid;
+    const int sslots = cfg.tier_bytes / (8 * P.sw);
+    int cur = -1;
+    uint32_t new_groups = 0;
+    for (int64_t k = 0;; ++k) {
+        int s = (int)(k % cfg.stages);
+        uint32_t parity = (uint32_t)((k / cfg.stages) & 1);
+        if (!mbar_wait(&full[s], parity)) {
+            set_error(descs[0].ctrl, kErrTimeout);
+            break;
+        }
+        const StageHdr& h = hdr[s];
+        const int64_t tile = h.tile;
+        if (tile < 0) break;
+        const int inst = h.inst;
+        if (inst != cur) {  // uniform across consumer warps: they all see every tile
+            consumer_bar(NT);
+            if (cur >= 0) {
+                if (TIER == kTierDirect) {
+                    flush_direct(P, D, tier, tier + (size_t)P.direct_slots * P.hw * NT, NT, ctid);
+                } else {
+                    flush_hash<KW>(P, D, tier, D.smem_slots < sslots ? D.smem_slots : sslots, NT, ctid, new_groups,
+                                   cfg.g_probes);
+                }
+                if (new_groups) atomicAdd((unsigned long long*)&D.ctrl[CTRL_GROUPS], (unsigned long long)new_groups);
+                new_groups = 0;
+                consumer_bar(NT);
+            }
+            coop_copy(&D, &descs[inst], (int)sizeof(BatchDesc), ctid, NT);
+            zero_words(tier, cfg.tier_bytes / 8, ctid, NT);
+            consumer_bar(NT);
+            cur = inst;
+        }
+        const TileView& v = h.view;
+        const int rows = h.rows;
+        const int64_t row0 = h.row0;
+        if (TIER == kTierDirect) {
+            constexpr int R = 8;
+            for (int base = 0; base < rows; base += R * NT) {
+                int64_t r[R];
+                bool live[R];
+#pragma unroll
+                for (int j = 0; j < R; ++j) {
+                    r[j] = base + j * NT + ctid;
+                    live[j] = r[j] < rows && (v.sel == nullptr || bit_at(v.sel, r[j]));
+                }
+                direct_chunk<R>(P, D, v, r, live, tier, tier + (size_t)P.direct_slots * P.hw * NT, NT, ctid);
+            }
+        } else {
+            constexpr int R = 4;
+            const int ss = D.smem_slots < sslots ? D.smem_slots : sslots;
+            const bool wa = D.warp_agg != 0;
+            for (int base = 0; base < rows; base += R * NT) {  // uniform trip count: warps stay converged
+                int64_t r[R];
+                bool live[R];
+#pragma unroll
+                for (int j = 0; j < R; ++j) {
+                    r[j] = base + j * NT + ctid;
+                    live[j] = r[j] < rows && (v.sel == nullptr || bit_at(v.sel, r[j]));
+                }
+                hash_chunk<KW, R>(P, D, v, r, live, row0, tier, ss, cfg.s_probes, cfg.g_probes, wa, new_groups);
+            }
+        }
+        __syncwarp();
+        if ((ctid & 31) == 0) mbar_arrive(&empty[s]);
+    }
+    if (cur >= 0) {
+        consumer_bar(NT);
+        if (TIER == kTierDirect) {
+            flush_direct(P, D, tier, tier + (size_t)P.direct_slots * P.hw * NT, NT, ctid);
+        } else {
+            flush_hash<KW>(P, D, tier, D.smem_slots < sslots ? D.smem_slots : sslots, NT, ctid, new_groups,
+                           cfg.g_probes);
+        }
+        if (new_groups) atomicAdd((unsigned long long*)&D.ctrl[CTRL_GROUPS], (unsigned long long)new_groups);
+    }
+}
+
+}  // namespace vr

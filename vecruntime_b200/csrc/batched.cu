@@ -73,8 +73,8 @@ static int batched_enqueue(vr_batched* b, cudaStream_t st) {
         LaunchCfg L = b->cfg;
         L.total_tiles = b->total_tiles;
         L.num_desc = n;
-        if ((e = launch_aggregate(b->kw, b->tier, b->descs_dev, L, b->blocks, b->counter, st)) != cudaSuccess)
-            return VR_ERR_CUDA;
+        // every instance shares the program: the first instance's kernel serves all
+        if ((e = agg_launch(b->inst[0], b->descs_dev, L, b->blocks, b->counter, st)) != cudaSuccess) return VR_ERR_CUDA;
     } else {
         for (int i = 0; i < n; ++i) {
             vr_agg* h = b->inst[i];
@@ -85,8 +85,7 @@ static int batched_enqueue(vr_batched* b, cudaStream_t st) {
             LaunchCfg L = h->launch;
             L.total_tiles = d.num_tiles;
             int blocks = (int)std::min<int64_t>(h->blocks, d.num_tiles);
-            if ((e = launch_aggregate(h->plan.prog.kw, h->cfg.tier, b->descs_dev + i, L, blocks, &d.ctrl[CTRL_NEXT_TILE],
-                                      st)) != cudaSuccess)
+            if ((e = agg_launch(h, b->descs_dev + i, L, blocks, &d.ctrl[CTRL_NEXT_TILE], st)) != cudaSuccess)
                 return VR_ERR_CUDA;
         }
     }

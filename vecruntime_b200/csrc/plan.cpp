@@ -410,7 +410,7 @@ struct Builder {
                             return fail(VR_ERR_UNSUPPORTED, "product needs rounding (scale adjustment) - CPU path");
                         kind = OP_SUM_PROD;
                         w = add_op(kind, -1, -1, (f.flags & VR_FN_CHECKED) ? OPF_CHECKED : 0, &f);
-                        c = w + 7;  // the op counts its own non-null products
+                        c = w + 7;  // the op counts its null products: count = rows - nulls
                     } else {
                         if (!in) return fail(VR_ERR_INVALID, "decimal sum needs an input");
                         if (in->lane == VR_INT64 || in->lane == VR_INT32)
@@ -422,12 +422,14 @@ struct Builder {
                         w = add_op(kind, f.input, -1, 0, nullptr);
                         c = add_op(OP_COUNT_VALID, f.input, -1, 0, nullptr);
                     }
+                    const int nc = kind == OP_SUM_PROD ? OUTF_NULLCOUNT : 0;  // products count their nulls
                     if (f.kind == VR_FN_SUM_DECIMAL) {
-                        out(OUT_DEC_SUM, VR_DECIMAL128, dflags, kind, w, c, -1, f.precision, f.scale);
-                        out(OUT_IS_EMPTY, VR_BOOL, 0, 0, 0, c, -1, 0, 0);
+                        out(OUT_DEC_SUM, VR_DECIMAL128, dflags | nc, kind, w, c, -1, f.precision, f.scale);
+                        out(OUT_IS_EMPTY, VR_BOOL, nc, 0, 0, c, -1, 0, 0);
                     } else {
-                        out(OUT_DEC_SUM, VR_DECIMAL128, OUTF_ZERO_WHEN_EMPTY, kind, w, c, -1, f.precision, f.scale);
-                        out(OUT_COUNT, VR_INT64, 0, 0, c, 0, -1, 0, 0);
+                        out(OUT_DEC_SUM, VR_DECIMAL128, OUTF_ZERO_WHEN_EMPTY | nc, kind, w, c, -1, f.precision,
+                            f.scale);
+                        out(OUT_COUNT, VR_INT64, nc, 0, c, 0, -1, 0, 0);
                     }
                     break;
                 }
@@ -477,6 +479,16 @@ struct Builder {
         if (P.num_cols > kMaxCols) return fail(VR_ERR_UNSUPPORTED, "too many input columns");
         P.aw = words;
         P.sw = (P.kw + P.aw + 1) & ~1;
+        // direct tier: hot words per op (the running values every row touches)
+        P.hw = 0;
+        for (int i = 0; i < P.num_ops; ++i) {
+            OpDesc& o = P.ops[i];
+            int hot = 1;
+            if (o.kind == OP_SUM_F64 || o.kind == OP_SUM_D128 || o.kind == OP_MAX_D128) hot = 2;
+            if (o.kind == OP_MERGE_DSUM || o.kind == OP_MERGE_DAVG) hot = 3;
+            o.hword = (int16_t)P.hw;
+            P.hw += hot;
+        }
         if (P.direct_slots == 0 && spec.num_keys == 0) P.direct_slots = 1;
         if (spec.num_keys == 0) plan.direct_ok = true;
         return VR_OK;

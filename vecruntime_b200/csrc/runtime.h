@@ -54,6 +54,8 @@ struct StageSlot {
     int64_t rows = 0;
 };
 
+struct JitKernel;
+
 struct DeviceInfo {
     int sms = 148;
     int smem_optin = 232448;
@@ -108,6 +110,8 @@ struct vr_agg {
     vr_agg_stats stats{};
     bool trace = false;
     bool dead = false;
+    vr::JitKernel* jit = nullptr;  // the spec's own kernel (owned by the process-wide cache)
+    std::string jit_error;         // why it could not be compiled, when it could not
 };
 
 namespace vr {
@@ -118,6 +122,8 @@ int agg_build(const vr_agg_spec* spec, const vr_tune_choice* forced, vr_agg** ou
 // Fills a BatchDesc for a device-resident batch (no copies).
 void fill_desc(vr_agg* h, const vr_batch& b, BatchDesc& d, uint64_t* ctrl, const StageSlot& s, int64_t tile_begin);
 int agg_resolve_all(vr_agg* h);
+cudaError_t agg_launch(vr_agg* h, const BatchDesc* descs, const LaunchCfg& L, int blocks, uint64_t* tile_counter,
+                       cudaStream_t st);
 int64_t tiles_for(const vr_agg* h, int64_t rows);
 void set_thread_error(const std::string& msg);
 }  // namespace vr

@@ -11,7 +11,9 @@
 //     used both to apply one row's contribution and to merge a whole state
 //     (shared-memory tier flush, rehash, partial merges).
 #pragma once
+#ifndef __CUDACC_RTC__
 #include <stdint.h>
+#endif
 
 #include "vrgpu.h"
 
@@ -68,7 +70,7 @@ struct OpDesc {
     int8_t nterms;
     int8_t prec;      // OP_SUM_PROD: product precision (rows reaching 10^prec are null / an error)
     int16_t word;     // first accumulator word
-    int16_t pad1;
+    int16_t hword;    // direct tier: first thread-private hot word
     int8_t term_col[3];
     int8_t term_sign[3];
     int16_t pad2;
@@ -102,6 +104,7 @@ struct Program {
     int32_t lock_mode;               // kw > 2: claim/publish protocol instead of one CAS
     int32_t aw;                      // accumulator words
     int32_t sw;                      // slot stride in words (kw + aw, even)
+    int32_t hw;                      // direct tier: thread-private hot words per group
     int32_t num_ops;
     OpDesc ops[kMaxOps];
     uint8_t word_kind[kMaxAccWords];
@@ -176,6 +179,7 @@ enum OutFlags : uint8_t {
     OUTF_MIN = 8,
     OUTF_FROM_FLAGS = 16,      // OUT_IS_EMPTY from a merge flags word
     OUTF_ZERO_WHEN_EMPTY = 32, // decimal buffer: zero (valid) for an empty group
+    OUTF_NULLCOUNT = 64,       // the count is rows (word 0) minus a null count word
 };
 
 struct OutDesc {

@@ -51,6 +51,7 @@ VR_SPEC_NO_WARP_AGG = 8
 VR_SPEC_WARP_AGG = 16
 VR_SPEC_NO_TMA = 32
 VR_SPEC_TRACE = 64
+VR_SPEC_NO_JIT = 128
 
 VR_HOST, VR_DEVICE = 0, 1
 VR_BATCHED_PERSISTENT, VR_BATCHED_PLAIN = 0, 1
@@ -104,7 +105,8 @@ class AggStats(C.Structure):
                 ("batches", C.c_int64), ("rehashes", C.c_int64), ("deferred_rows", C.c_int64),
                 ("threads", C.c_int32), ("blocks", C.c_int32), ("smem_bytes", C.c_int32),
                 ("tile_rows", C.c_int32), ("last_kernel_ms", C.c_double), ("total_kernel_ms", C.c_double),
-                ("total_h2d_ms", C.c_double), ("total_d2h_ms", C.c_double), ("kernel_launches", C.c_int64)]
+                ("total_h2d_ms", C.c_double), ("total_d2h_ms", C.c_double), ("kernel_launches", C.c_int64),
+                ("jit", C.c_int32), ("reserved", C.c_int32)]
 
 
 class TuneChoice(C.Structure):
@@ -170,6 +172,7 @@ PROTOTYPES = [
     ("vr_tune_save", C.c_int, [C.c_char_p]),
     ("vr_tune_search", C.c_int, [C.POINTER(AggSpec), C.POINTER(Batch), C.c_int32, C.POINTER(TuneChoice),
                                  C.POINTER(C.c_double)]),
+    ("vr_jit_compile", C.c_int, [C.POINTER(AggSpec), C.c_int32, C.POINTER(C.c_int64), C.c_char_p, C.c_size_t]),
     ("vr_agg_plan", C.c_int, [C.POINTER(AggSpec), C.POINTER(PlanInfo), C.POINTER(ColumnType), C.c_int32]),
     ("vr_srv_create", C.c_int, [C.POINTER(SrvConfig), C.POINTER(_P)]),
     ("vr_srv_open_query", C.c_int, [_P, C.POINTER(AggSpec), C.POINTER(C.c_int32)]),
