@@ -268,6 +268,17 @@ int vr_host_unregister(void* p);
  *      kernels/.../HashKernels.java:42-236). Device pointers; out[n]. ------ */
 int vr_hash_rows(int32_t num_keys, const vr_column_type* types, const vr_column* keys,
                  int64_t num_rows, uint32_t* out_device, int32_t finish, void* stream);
+/* vr_hash_rows without any device allocation, for callers that must not
+ * allocate (a serving thread whose cudaMalloc/cudaFree would synchronise the
+ * device under other queries, an executor at its memory cap). No counterpart
+ * in the reference, whose hashing runs on the JVM heap. The key descriptors go
+ * to a fixed 640-byte device scratch inside the library: at most 16 key
+ * columns, more is VR_ERR_INVALID. Enqueues on `stream` and returns without
+ * waiting. Calls on one stream are ordered; calls that overlap in time on
+ * other streams or threads share the scratch and race. The first call on a
+ * device looks the scratch up; make it before any stream capture. */
+int vr_hash_rows_noalloc(int32_t num_keys, const vr_column_type* types, const vr_column* keys,
+                         int64_t num_rows, uint32_t* out_device, int32_t finish, void* stream);
 
 /* ---- batched persistent aggregation ------------------------------------
  * Many independent instances (Spark tasks' batches) in one persistent

@@ -996,6 +996,55 @@ int vr_hash_rows(int32_t num_keys, const vr_column_type* types, const vr_column*
     return VR_OK;
 }
 
+// The same kernel as vr_hash_rows with its descriptor table in the library's
+// fixed device scratch instead of cudaMalloc'd memory. Meant for callers that
+// must not allocate: cudaMalloc/cudaFree can synchronise the whole device
+// (stalling a serving thread's other queries) and a memory-capped executor
+// may have no device memory left to hand out. The scratch address is looked
+// up once per device and kept; calls enqueue on `stream` and return.
+int vr_hash_rows_noalloc(int32_t num_keys, const vr_column_type* types, const vr_column* keys, int64_t num_rows,
+                         uint32_t* out_device, int32_t finish, void* stream) {
+    if (num_keys < 0 || (num_keys > 0 && (!types || !keys)) || !out_device) {
+        t_last_error = "vr_hash_rows_noalloc: null descriptor or output pointer, or a negative key count";
+        return VR_ERR_INVALID;
+    }
+    if (num_keys > kHashRowsScratchMaxKeys) {
+        t_last_error = "vr_hash_rows_noalloc: " + std::to_string(num_keys) + " key columns exceed its fixed scratch of " +
+                       std::to_string(kHashRowsScratchMaxKeys);
+        return VR_ERR_INVALID;
+    }
+    static std::mutex mu;
+    static void* scratch_of[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess && (dev < 0 || dev >= 64)) {
+        t_last_error = "vr_hash_rows_noalloc: device index above 63";
+        return VR_ERR_UNSUPPORTED;
+    }
+    char* scratch = nullptr;
+    if (e == cudaSuccess) {
+        std::lock_guard<std::mutex> lk(mu);
+        if (!scratch_of[dev]) {
+            void* p = nullptr;
+            e = hash_rows_scratch_address(&p);
+            if (e == cudaSuccess) scratch_of[dev] = p;
+        }
+        scratch = static_cast<char*>(scratch_of[dev]);
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    vr_column_type* td = reinterpret_cast<vr_column_type*>(scratch);
+    vr_column* kd = reinterpret_cast<vr_column*>(scratch + kHashRowsScratchKeysOffset);
+    if (e == cudaSuccess && num_keys > 0)
+        e = cudaMemcpyAsync(td, types, sizeof(vr_column_type) * num_keys, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && num_keys > 0) e = cudaMemcpyAsync(kd, keys, sizeof(vr_column) * num_keys, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = launch_hash_rows(num_keys, td, kd, num_rows, out_device, finish, st);
+    if (e != cudaSuccess) {
+        t_last_error = cudaGetErrorString(e);
+        return VR_ERR_CUDA;
+    }
+    return VR_OK;
+}
+
 int vr_jit_compile(const vr_agg_spec* spec, int32_t tier, int64_t* cubin_bytes, char* log, size_t cap) {
     if (!spec) return VR_ERR_INVALID;
     Plan plan;

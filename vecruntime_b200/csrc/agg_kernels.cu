@@ -543,4 +543,15 @@ cudaError_t launch_hash_rows(int num_keys, const vr_column_type* types_dev, cons
     return cudaGetLastError();
 }
 
+// Fixed device scratch for vr_hash_rows_noalloc: the key-column descriptors
+// of one call (types first, then columns), so that entry point never has to
+// allocate the small table the kernel reads. One copy per device, shared by
+// every call on that device. Nothing here needs to start at zero: each call
+// writes the descriptors it uses before its kernel reads them.
+static __device__ __align__(256) unsigned char g_hash_rows_scratch[kHashRowsScratchBytes];
+
+cudaError_t hash_rows_scratch_address(void** out) {
+    return cudaGetSymbolAddress(out, g_hash_rows_scratch);
+}
+
 }  // namespace vr

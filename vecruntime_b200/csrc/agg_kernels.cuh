@@ -31,6 +31,16 @@ cudaError_t launch_compact_kw(int kw, const uint64_t* table, int64_t slots, int 
 cudaError_t launch_emit(const Program* prog_dev, const EmitProgram* emit_dev, const uint64_t* table,
                         const int64_t* slot_of, int64_t from, int64_t to, const vr_out_column* outs_dev,
                         uint64_t* ctrl, cudaStream_t stream);
+// vr_hash_rows_noalloc's fixed scratch: at most this many key columns, their
+// vr_column_type entries at offset 0 and vr_column entries at
+// kHashRowsScratchKeysOffset.
+constexpr int kHashRowsScratchMaxKeys = 16;
+constexpr size_t kHashRowsScratchKeysOffset = kHashRowsScratchMaxKeys * sizeof(vr_column_type);
+constexpr size_t kHashRowsScratchBytes = kHashRowsScratchKeysOffset + kHashRowsScratchMaxKeys * sizeof(vr_column);
+static_assert(kHashRowsScratchBytes == 640, "the header documents a 640-byte scratch");
+// The scratch's device address on the current device.
+cudaError_t hash_rows_scratch_address(void** out);
+
 // Reference row hash (HashKernels.java) over device key columns.
 cudaError_t launch_hash_rows(int num_keys, const vr_column_type* types_dev, const vr_column* keys_dev,
                              int64_t n, uint32_t* out, int finish, cudaStream_t stream);

@@ -163,6 +163,8 @@ PROTOTYPES = [
     ("vr_host_register", C.c_int, [_P, C.c_size_t]),
     ("vr_host_unregister", C.c_int, [_P]),
     ("vr_hash_rows", C.c_int, [C.c_int32, C.POINTER(ColumnType), C.POINTER(Column), C.c_int64, _P, C.c_int32, _P]),
+    ("vr_hash_rows_noalloc", C.c_int, [C.c_int32, C.POINTER(ColumnType), C.POINTER(Column), C.c_int64, _P, C.c_int32,
+                                       _P]),
     ("vr_batched_create", C.c_int, [C.POINTER(BatchedPlan), C.POINTER(_P)]),
     ("vr_batched_run", C.c_int, [_P, _P]),
     ("vr_batched_destroy", None, [_P]),
