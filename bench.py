@@ -23,7 +23,6 @@ import argparse
 import ctypes as C
 import json
 import os
-import subprocess
 import sys
 import threading
 import time
@@ -50,55 +49,74 @@ def measured_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clock and clock-event reasons of the GPU under test, polled through
+    NVML every ~2 ms while the timed region runs (nvidia-smi's fastest period
+    is longer than a short timed region). The GPU is found by PCI bus id, so
+    the CUDA index and the NVML index may differ."""
 
-    def __init__(self, index: int):
-        self.index = index
-        self.rows = []
-        self.proc = None
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20,
+               "sw_power_cap": 0x4, "hw_power_brake_slowdown": 0x80}
+
+    def __init__(self, cuda_index: int, period_s: float = 0.002):
+        self.cuda_index = cuda_index
+        self.period = period_s
+        self.rows = []  # (sm_mhz, reasons bitmask)
+        self.max_mhz = None
+        self.error = None
+        self._stop = threading.Event()
+        self._t = None
+
+    def _handle(self):
+        import pynvml
+        import torch
+
+        pynvml.nvmlInit()
+        p = torch.cuda.get_device_properties(self.cuda_index)
+        bus = "%08x:%02x:%02x.0" % (p.pci_domain_id, p.pci_bus_id, p.pci_device_id)
+        return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
 
     def __enter__(self):
-        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
-        except (FileNotFoundError, OSError):
-            self.proc = None
+            self.nvml, self.h = self._handle()
+            self.max_mhz = self.nvml.nvmlDeviceGetMaxClockInfo(self.h, self.nvml.NVML_CLOCK_SM)
+            self._sample()
+            self._t = threading.Thread(target=self._loop, daemon=True)
+            self._t.start()
+        except Exception as e:  # no NVML: the line says so instead of a number
+            self.error = f"{type(e).__name__}: {e}"
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.rows.append([x.strip() for x in line.split(",")])
+    def _sample(self):
+        sm = self.nvml.nvmlDeviceGetClockInfo(self.h, self.nvml.NVML_CLOCK_SM)
+        reasons = self.nvml.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+        self.rows.append((sm, reasons))
+
+    def _loop(self):
+        while not self._stop.is_set():
+            try:
+                self._sample()
+            except Exception as e:
+                self.error = f"{type(e).__name__}: {e}"
+                return
+            time.sleep(self.period)
 
     def __exit__(self, *exc):
-        if self.proc:
-            self.proc.terminate()
+        self._stop.set()
+        if self._t is not None:
+            self._t.join(timeout=5)
             try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
+                self._sample()
+            except Exception:
+                pass
 
     def summary(self):
-        sm = []
-        mx = None
-        reasons = set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in self.rows:
-            try:
-                sm.append(float(r[1]))
-                mx = float(r[2])
-            except (ValueError, IndexError):
-                continue
-            for name, val in zip(names, r[5:9]):
-                if val.strip().lower() == "active":
-                    reasons.add(name)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        sm = [r[0] for r in self.rows]
+        reasons = sorted({name for _, bits in self.rows for name, bit in self.REASONS.items() if bits & bit})
+        out = {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": self.max_mhz, "reasons": reasons,
+               "samples": len(sm), "source": "nvml, polled every %.0f ms during the timed region" % (self.period * 1e3)}
+        if self.error:
+            out["error"] = self.error
+        return out
 
 
 # ------------------------------------------------------------------ workloads
@@ -260,10 +278,11 @@ def run_ours(args, rank, world, device):
 
 
 def workload_label(w):
-    return {"decimal": "low-cardinality decimal report: 60M rows, 2 dictionary keys (3x2 -> 6 groups), "
+    n = f"{w.rows // 1_000_000}M rows" if w.rows % 1_000_000 == 0 else f"{w.rows:,} rows"
+    return {"decimal": f"low-cardinality decimal report: {n}, 2 dictionary keys (3x2 -> 6 groups), "
                        "4 DECIMAL(12,2) columns, exact decimal(38,6) sums",
-            "plain": "plain grouped aggregation: 1,048,576 rows, int64 key over 1,000 values, 5% nulls",
-            "highcard": "high-cardinality composite key: 100M rows, Zipf(1.1) int64 x int32[16], 1% null keys"
+            "plain": f"plain grouped aggregation: {n}, int64 key over 1,000 values, 5% nulls",
+            "highcard": f"high-cardinality composite key: {n}, Zipf(1.1) int64 x int32[16], 1% null keys"
             }.get(w.name, w.name)
 
 

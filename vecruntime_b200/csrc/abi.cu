@@ -130,20 +130,26 @@ static int choose_config(vr_agg* h, const vr_tune_choice* forced) {
     };
     bool chosen = false;
     if (h->plan.direct_ok && (want_tier == -1 || want_tier == 0)) {
+        // A tile is exactly one chunk: threads x R rows (R rows per consumer
+        // thread), so no lane idles inside a full tile. More consumer warps
+        // first, then longer tiles.
         const int nts[] = {256, 192, 128, 96, 64};
-        const int Ts[] = {2048, 1024, 512};
+        const int Rs[] = {8, 4, 2};
         for (int nt : nts) {
             if (forced && forced->threads && nt != forced->threads) continue;
             // thread-private hot words + the CTA's cold words
             int64_t tb = (P.direct_slots * P.hw * (int64_t)nt + P.direct_slots * P.aw) * 8;
             if (tb > budget) continue;
-            for (int T : Ts) {
+            for (int R : Rs) {
+                const int T = nt * R;
+                if (T % 128) continue;
                 if (forced && forced->tile_rows && T != forced->tile_rows) continue;
                 for (int st = 3; st >= 2 && !chosen; --st) {
                     if (fits(st, T, (int)tb)) {
                         c.tier = kTierDirect;
                         c.threads = nt;
                         c.tile_rows = T;
+                        c.rchunk = R;
                         c.stages = st;
                         chosen = true;
                     }
@@ -164,6 +170,7 @@ static int choose_config(vr_agg* h, const vr_tune_choice* forced) {
         c.stages = 3;
         while (c.stages > 2 && !fits(c.stages, c.tile_rows, 0)) --c.stages;
         while (!fits(c.stages, c.tile_rows, 0) && c.tile_rows > 256) c.tile_rows /= 2;
+        c.rchunk = c.tile_rows >= 4 * c.threads ? 4 : 2;
         int free_bytes = budget - smem_map(c.stages, stage_bytes_for(P, c.tile_rows), 0).total;
         int max_slots = free_bytes > 0 ? free_bytes / (8 * P.sw) : 0;
         int slots = 1;
@@ -173,6 +180,10 @@ static int choose_config(vr_agg* h, const vr_tune_choice* forced) {
             int64_t need = next_pow2(std::max<int64_t>(64, 2 * (est > 0 ? est : 1 << 30)));
             if (need <= slots) {
                 c.smem_slots = (int)need;  // every group fits: a private table per CTA
+            } else if (est > 0 && est > 64 * (int64_t)slots && want_tier != 1) {
+                // far more groups than a CTA can cache: most rows would miss
+                // the cache after probing it, so go to HBM directly
+                c.smem_slots = 0;
             } else {
                 c.smem_slots = std::min(slots, 2048);  // hot-key cache in front of HBM
             }
@@ -203,6 +214,7 @@ static int choose_config(vr_agg* h, const vr_tune_choice* forced) {
     LaunchCfg& L = h->launch;
     std::memset(&L, 0, sizeof(L));
     L.tile_rows = c.tile_rows;
+    L.rchunk = c.rchunk;
     L.stages = c.stages;
     L.consumer_threads = c.threads;
     L.num_desc = 1;
@@ -326,7 +338,7 @@ int agg_build(const vr_agg_spec* spec, const vr_tune_choice* forced, vr_agg** ou
     // interpreted ahead-of-time kernel stays the fallback
     if (jit_enabled() && !(spec->flags & VR_SPEC_NO_JIT)) {
         std::string why;
-        h->jit = jit_get(h->plan.prog, h->plan.prog.kw, h->cfg.tier, h->device, &why);
+        h->jit = jit_get(h->plan.prog, h->plan.prog.kw, h->cfg.tier, h->cfg.rchunk, h->device, &why);
         if (h->jit) {
             int regs = jit_regs(h->jit);
             const DeviceInfo& di = device_info(h->device);
@@ -1055,7 +1067,7 @@ int vr_jit_compile(const vr_agg_spec* spec, int32_t tier, int64_t* cubin_bytes, 
     }
     size_t bytes = 0;
     std::string err;
-    bool ok = jit_compile_only(plan.prog, plan.prog.kw, tier == 0 ? kTierDirect : kTierHash, &bytes, &err);
+    bool ok = jit_compile_only(plan.prog, plan.prog.kw, tier == 0 ? kTierDirect : kTierHash, 4, &bytes, &err);
     if (log && cap) std::snprintf(log, cap, "%s", err.c_str());
     if (cubin_bytes) *cubin_bytes = (int64_t)bytes;
     return ok ? VR_OK : VR_ERR_UNSUPPORTED;

@@ -420,6 +420,39 @@ VR_DEV void zero_words(uint64_t* p, int64_t n, int tid, int nt) {
     for (int64_t i = tid; i < n; i += nt) p[i] = 0;
 }
 
+// One staged tile of `rows` rows, in chunks of R rows per consumer thread
+// (row base + j * NT + ctid for j < R). The host sizes direct-tier tiles to
+// exactly NT * R rows, so a full tile is one chunk with every lane busy.
+template <int KW, int TIER, int R>
+VR_DEV void consume_tile(const Program& P, const BatchDesc& D, const LaunchCfg& cfg, const TileView& v, int rows,
+                         int64_t row0, uint64_t* tier, int sslots, int NT, int ctid, uint32_t& new_groups) {
+    if (TIER == kTierDirect) {
+        for (int base = 0; base < rows; base += R * NT) {
+            int64_t r[R];
+            bool live[R];
+#pragma unroll
+            for (int j = 0; j < R; ++j) {
+                r[j] = base + j * NT + ctid;
+                live[j] = r[j] < rows && (v.sel == nullptr || bit_at(v.sel, r[j]));
+            }
+            direct_chunk<R>(P, D, v, r, live, tier, tier + (size_t)P.direct_slots * P.hw * NT, NT, ctid);
+        }
+    } else {
+        const int ss = D.smem_slots < sslots ? D.smem_slots : sslots;
+        const bool wa = D.warp_agg != 0;
+        for (int base = 0; base < rows; base += R * NT) {  // uniform trip count: warps stay converged
+            int64_t r[R];
+            bool live[R];
+#pragma unroll
+            for (int j = 0; j < R; ++j) {
+                r[j] = base + j * NT + ctid;
+                live[j] = r[j] < rows && (v.sel == nullptr || bit_at(v.sel, r[j]));
+            }
+            hash_chunk<KW, R>(P, D, v, r, live, row0, tier, ss, cfg.s_probes, cfg.g_probes, wa, new_groups);
+        }
+    }
+}
+
 // ---------------------------------------------------------- the kernel ---
 // The kernel body; the ahead-of-time kernel (agg_kernels.cu) and the per-spec
 // kernels compiled at run time (jit.cpp) both wrap it.
@@ -490,35 +523,15 @@ VR_DEV void aggregate_body(const BatchDesc* __restrict__ descs, const LaunchCfg&
             cur = inst;
         }
         const TileView& v = h.view;
-        const int rows = h.rows;
-        const int64_t row0 = h.row0;
-        if (TIER == kTierDirect) {
-            constexpr int R = 8;
-            for (int base = 0; base < rows; base += R * NT) {
-                int64_t r[R];
-                bool live[R];
-#pragma unroll
-                for (int j = 0; j < R; ++j) {
-                    r[j] = base + j * NT + ctid;
-                    live[j] = r[j] < rows && (v.sel == nullptr || bit_at(v.sel, r[j]));
-                }
-                direct_chunk<R>(P, D, v, r, live, tier, tier + (size_t)P.direct_slots * P.hw * NT, NT, ctid);
-            }
-        } else {
-            constexpr int R = 4;
-            const int ss = D.smem_slots < sslots ? D.smem_slots : sslots;
-            const bool wa = D.warp_agg != 0;
-            for (int base = 0; base < rows; base += R * NT) {  // uniform trip count: warps stay converged
-                int64_t r[R];
-                bool live[R];
-#pragma unroll
-                for (int j = 0; j < R; ++j) {
-                    r[j] = base + j * NT + ctid;
-                    live[j] = r[j] < rows && (v.sel == nullptr || bit_at(v.sel, r[j]));
-                }
-                hash_chunk<KW, R>(P, D, v, r, live, row0, tier, ss, cfg.s_probes, cfg.g_probes, wa, new_groups);
-            }
+#ifdef VR_JIT
+        consume_tile<KW, TIER, VR_JIT_RCHUNK>(P, D, cfg, v, h.rows, h.row0, tier, sslots, NT, ctid, new_groups);
+#else
+        switch (cfg.rchunk) {  // uniform
+            case 8: consume_tile<KW, TIER, 8>(P, D, cfg, v, h.rows, h.row0, tier, sslots, NT, ctid, new_groups); break;
+            case 2: consume_tile<KW, TIER, 2>(P, D, cfg, v, h.rows, h.row0, tier, sslots, NT, ctid, new_groups); break;
+            default: consume_tile<KW, TIER, 4>(P, D, cfg, v, h.rows, h.row0, tier, sslots, NT, ctid, new_groups);
         }
+#endif
         __syncwarp();
         if ((ctid & 31) == 0) mbar_arrive(&empty[s]);
     }

@@ -255,9 +255,10 @@ bool jit_enabled() {
     return !(e && std::strcmp(e, "0") == 0);
 }
 
-static std::string jit_source(const Program& P, int kw, int tier) {
+static std::string jit_source(const Program& P, int kw, int tier, int rchunk) {
     std::string src = kPrelude;
     src += "#define VR_JIT_KW " + std::to_string(kw) + "\n#define VR_JIT_TIER " + std::to_string(tier) + "\n";
+    src += "#define VR_JIT_RCHUNK " + std::to_string(rchunk) + "\n";
     src += "#define VR_JIT_NUM_OPS " + std::to_string(P.num_ops) + "\n";
     src += "#include \"agg_device.cuh\"\nnamespace vr {\n__constant__ const Program kJitProg = ";
     src += program_literal(P);
@@ -273,15 +274,15 @@ static std::string jit_source(const Program& P, int kw, int tier) {
     return src;
 }
 
-bool jit_compile_only(const Program& P, int kw, int tier, size_t* cubin_bytes, std::string* err) {
+bool jit_compile_only(const Program& P, int kw, int tier, int rchunk, size_t* cubin_bytes, std::string* err) {
     std::vector<char> cubin;
-    if (!compile_cubin(jit_source(P, kw, tier), cubin, err)) return false;
+    if (!compile_cubin(jit_source(P, kw, tier, rchunk), cubin, err)) return false;
     if (cubin_bytes) *cubin_bytes = cubin.size();
     return true;
 }
 
-JitKernel* jit_get(const Program& P, int kw, int tier, int device, std::string* err) {
-    std::string src = jit_source(P, kw, tier);
+JitKernel* jit_get(const Program& P, int kw, int tier, int rchunk, int device, std::string* err) {
+    std::string src = jit_source(P, kw, tier, rchunk);
     uint64_t h = fnv64(src);
     for (int i = 0; i < jitsrc::kNum; ++i) h ^= fnv64(jitsrc::kTexts[i]) * (i + 3);
     std::lock_guard<std::mutex> lk(g_mu);

@@ -14,13 +14,13 @@ struct JitKernel;
 // (cached per process, and on disk under $VRGPU_JIT_CACHE when set).
 // Returns nullptr (with `err` set) when NVRTC or the driver is unavailable or
 // the compile fails; callers then use the ahead-of-time kernel.
-JitKernel* jit_get(const Program& prog, int kw, int tier, int device, std::string* err);
+JitKernel* jit_get(const Program& prog, int kw, int tier, int rchunk, int device, std::string* err);
 int jit_regs(const JitKernel* k);
 cudaError_t jit_launch(JitKernel* k, const BatchDesc* descs, const LaunchCfg& cfg, int blocks, uint64_t* tile_counter,
                        cudaStream_t stream);
 // Whether per-spec compilation is enabled ($VRGPU_JIT != "0").
 bool jit_enabled();
 // Compiles (NVRTC only, no device needed) and reports the cubin size.
-bool jit_compile_only(const Program& prog, int kw, int tier, size_t* cubin_bytes, std::string* err);
+bool jit_compile_only(const Program& prog, int kw, int tier, int rchunk, size_t* cubin_bytes, std::string* err);
 
 }  // namespace vr

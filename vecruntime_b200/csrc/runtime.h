@@ -21,6 +21,7 @@ struct Config {
     int threads = 256;        // consumer threads
     int blocks_per_sm = 1;
     int tile_rows = 2048;
+    int rchunk = 4;           // rows per consumer thread per chunk
     int stages = 2;
     int smem_slots = 0;       // hash tier shared cache
     int tma = 1;
