@@ -96,3 +96,49 @@ def test_high_cardinality_small_with_growth(cuda):
 def test_high_cardinality_small_warp_agg(cuda):
     w = G.high_cardinality(rows=400_000, domain=200_000)
     check(w, [w.batch()], flags=N.VR_SPEC_WARP_AGG)
+
+
+@pytest.mark.parametrize("finish", [1, 0])
+def test_row_hash_matches_the_oracle(cuda, finish):
+    """vr_hash_rows against the oracle's restatement of HashKernels
+    (HashKernels.java:42-236): every lane, nulls mixing NULL_MARK, NaN and
+    signed zeros in doubles, both limbs of DECIMAL128."""
+    import ctypes as C
+
+    from oracle.pyoracle import hash_rows
+
+    torch = cuda
+    rng = np.random.default_rng(4242)
+    n = 10_007
+    nulls = lambda p: rng.random(n) < p
+    d = rng.normal(size=n)
+    d[rng.random(n) < 0.05] = np.nan
+    d[rng.random(n) < 0.05] = -0.0
+    d[rng.random(n) < 0.05] = 0.0
+    cols = [Cc.ints(rng.integers(-2**31, 2**31, n), nulls(0.1), nullable=True),
+            Cc.longs(rng.integers(-2**63, 2**63 - 1, n, dtype=np.int64), nulls(0.05), nullable=True),
+            Cc.doubles(d, nulls(0.02), nullable=True),
+            Cc.bools(rng.random(n) < 0.5, nulls(0.1), nullable=True),
+            Cc.decimals128([int(x) * (1 << 64) + int(y) for x, y in zip(rng.integers(-2**62, 2**62, n),
+                                                                        rng.integers(0, 2**63, n))],
+                           38, 0, nulls(0.1), nullable=True),
+            Cc.dict_ids(rng.integers(0, 1000, n), 1000, nulls(0.01), nullable=True)]
+    want = hash_rows(cols, n, finish=bool(finish))
+    keep = []
+    types = (N.ColumnType * len(cols))(*[c.ctype() for c in cols])
+    dev = (N.Column * len(cols))()
+    for i, c in enumerate(cols):
+        t = torch.from_numpy(np.ascontiguousarray(c.data).view(np.uint8).copy()).cuda()
+        dev[i].data = t.data_ptr()
+        keep.append(t)
+        if c.validity is not None:
+            v = torch.from_numpy(np.ascontiguousarray(c.validity).copy()).cuda()
+            dev[i].validity = v.data_ptr()
+            keep.append(v)
+    out = torch.empty(n, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    rc = N.lib().vr_hash_rows(len(cols), types, dev, n, C.c_void_p(out.data_ptr()), finish, C.c_void_p(stream))
+    assert rc == N.VR_OK, N.lib().vr_thread_last_error()
+    torch.cuda.synchronize()
+    got = out.cpu().numpy().view(np.uint32)
+    assert np.array_equal(got, want), f"{int((got != want).sum())} of {n} hashes differ"

@@ -267,7 +267,7 @@ struct Builder {
                 std::memset(&kf, 0, sizeof(kf));
                 kf.col = (int8_t)stage(spec.key_columns[f.idx]);
                 kf.lane = (uint8_t)f.lane;
-                kf.bits = (int8_t)f.bits;
+                kf.bits = (uint8_t)f.bits;
                 kf.null_word = -1;
                 if (f.bits >= 64) {
                     kf.word = (int8_t)next_ded;

@@ -82,7 +82,7 @@ struct KeyField {
     uint8_t lane;
     int8_t word;       // data placement
     int8_t shift;
-    int8_t bits;       // 1, 32, 64 or 128
+    uint8_t bits;      // 1, 32, 64 or 128 (unsigned: 128 does not fit an int8_t)
     int8_t null_word;  // -1 when not nullable
     int8_t null_shift;
     uint8_t pad;
