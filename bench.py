@@ -39,6 +39,14 @@ def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
 
+# DRAM bytes (read + write) per row of the aggregate kernel, from one ncu
+# capture of an 8M-row launch (profiles/aggregate_decimal_report_8M.md:
+# 320.116 MB read + 3.576 MB written). The decimal report's traffic is its
+# input plus a fixed flush, so it scales with rows; the hash workloads' table
+# traffic does not (it follows the group count), so they report none.
+TRAFFIC_BYTES_PER_ROW = {"decimal": (320.116480e6 + 3.576064e6) / 8_000_000}
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -289,7 +297,11 @@ def run_ours(args, rank, world, device):
                    "l2": "inputs larger than L2 (%.2f GB > 126 MB)" % (in_bytes / 1e9),
                    "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": (TRAFFIC_BYTES_PER_ROW[w.name] * w.rows / 1e9
+                                 if w.name in TRAFFIC_BYTES_PER_ROW else None),
+                     "traffic_unit": "GB per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum, "
+                                     "8M-row capture scaled by rows)",
                      "algorithmic_bytes_per_launch": alg_bytes, "kernel_ms": kernel_ms},
         "e2e": e2e,
         "gpu_launches": launches,
