@@ -335,7 +335,8 @@ int vr_agg_plan(const vr_agg_spec* spec, vr_plan_info* info, vr_column_type* out
 
 /* Compiles the spec's specialised aggregate kernel for `tier` (0 direct,
  * 1 hash) with NVRTC -- host only, no GPU needed -- and reports the cubin
- * size; on failure the compiler log goes to `log`. */
+ * size; `log` receives the compiler log: the error on failure, ptxas's
+ * resource usage (registers, spills, local memory) on success. */
 int vr_jit_compile(const vr_agg_spec* spec, int32_t tier, int64_t* cubin_bytes, char* log, size_t cap);
 /* 1 and the recorded choice when the tuner has one for (spec, rows), else 0. */
 int vr_tune_lookup(const vr_agg_spec* spec, int64_t rows, vr_tune_choice* out);

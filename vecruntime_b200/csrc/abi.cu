@@ -630,11 +630,23 @@ int agg_resolve_all(vr_agg* h) {
     return VR_OK;
 }
 
+// A column the spec declares non-nullable must not bring a validity bitmap:
+// the kernels skip the validity test for such columns.
+const char* batch_nullability_error(const vr_agg* h, const vr_batch& b) {
+    for (int c = 0; c < h->plan.prog.num_cols; ++c) {
+        const int sc = h->plan.spec_of_staged[c];
+        if (!h->columns[sc].nullable && b.columns[sc].validity)
+            return "a column declared non-nullable carries a validity bitmap";
+    }
+    return nullptr;
+}
+
 static int agg_update(vr_agg* h, const vr_batch* b) {
     if (h->dead) return VR_ERR_STATE;
     if (!b || b->num_rows < 0 || (b->num_rows > 0 && !b->columns))
         return set_err(h, VR_ERR_INVALID, "bad batch");
     if (b->num_rows == 0) return VR_OK;
+    if (const char* why = batch_nullability_error(h, *b)) return set_err(h, VR_ERR_INVALID, why);
     cudaError_t e = cudaSetDevice(h->device);
     if (e != cudaSuccess) return cuda_err(h, e, "cudaSetDevice");
     StageSlot& s = h->slot[h->next_slot];

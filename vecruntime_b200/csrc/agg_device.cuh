@@ -430,8 +430,8 @@ VR_DEV void or_word(uint64_t (&k)[KW], int idx, uint64_t v) {
 // One key field of row r into the packed words (null: its null bit only).
 template <int KW>
 VR_DEV void pack_field(const KeyField& kf, const TileView& v, int64_t r, uint64_t (&k)[KW], bool& bad) {
-    if (!col_valid(v, kf.col, r)) {
-        if (kf.null_word >= 0) or_word<KW>(k, kf.null_word, 1ull << kf.null_shift);
+    if (kf.null_word >= 0 && !col_valid(v, kf.col, r)) {  // only nullable keys carry a bitmap
+        or_word<KW>(k, kf.null_word, 1ull << kf.null_shift);
         return;
     }
     switch (kf.lane) {
@@ -484,7 +484,7 @@ VR_DEV void pack_key(const Program& P, const TileView& v, int64_t r, uint64_t (&
 // lies outside the declared dictionary (null is the field's last value).
 VR_DEV int64_t direct_field(const KeyField& kf, const TileView& v, int64_t r) {
     int64_t val;
-    if (!col_valid(v, kf.col, r)) {
+    if (kf.null_word >= 0 && !col_valid(v, kf.col, r)) {  // only nullable keys carry a bitmap
         val = kf.card - 1;
     } else if (kf.lane == VR_BOOL) {
         val = bit_at(reinterpret_cast<const uint32_t*>(v.data[kf.col]), r);
@@ -624,10 +624,48 @@ VR_DEV void czero(Contrib& x) { x.a = x.b = x.c = x.d = x.e = x.f = x.g = x.h = 
 VR_DEV uint64_t lo32(int64_t x) { return (uint64_t)(uint32_t)x; }
 VR_DEV uint64_t hi32(int64_t x) { return (uint64_t)(int64_t)(int32_t)(x >> 32); }
 
+// Validity of input column c of op o at row r: only columns the spec
+// declares nullable are tested (a non-nullable column never carries a bitmap).
+template <class V>
+VR_DEV bool in_valid(const OpDesc& o, const V& v, int c, int64_t r) {
+    return !(o.flags & OPF_NULLABLE) || col_valid(v, c, r);
+}
+
+// |p| < 10^prec for an int64 p (2^63 < 10^19: always true from 19 digits on).
+VR_DEV bool within_precision64(int64_t p, int prec) {
+    if (prec >= 19) return true;
+    const uint64_t m = p < 0 ? 0ull - (uint64_t)p : (uint64_t)p;
+    return m < c_pow10.lo[prec];
+}
+
+// The exact product a * b * c (c = 1 for two factors) of a decimal
+// product row whose int64 fast path gave up: int64, 128-bit, or null (past
+// 128 bits or the precision; `error` with ANSI). Out of line: rare rows.
+struct ProdResult {
+    enum { kInt64 = 0, kWide = 1, kNull = 2 };
+    uint64_t lo, hi;
+    uint32_t kind, error;
+};
+static __device__ __noinline__ ProdResult product_exact(int64_t a, int64_t b, int64_t c, int prec, bool checked) {
+    ProdResult s = {0, 0, ProdResult::kNull, checked ? 1u : 0u};
+    I128 p = mul_i64(a, b);
+    if (c != 1) {
+        I128 q;
+        if (!mul_i128_i64(p, c, q)) return s;
+        p = q;
+    }
+    if (!within_precision(p.lo, p.hi, prec)) return s;
+    s.error = 0;
+    s.lo = p.lo;
+    s.hi = (uint64_t)p.hi;
+    s.kind = p.hi == ((int64_t)p.lo >> 63) ? ProdResult::kInt64 : ProdResult::kWide;
+    return s;
+}
+
 template <class V>
 VR_DEV bool terms_valid(const OpDesc& o, const V& v, int64_t r) {
-    bool ok = col_valid(v, o.term_col[0], r) && col_valid(v, o.term_col[1], r);
-    if (o.nterms > 2) ok = ok && col_valid(v, o.term_col[2], r);
+    bool ok = in_valid(o, v, o.term_col[0], r) && in_valid(o, v, o.term_col[1], r);
+    if (o.nterms > 2) ok = ok && in_valid(o, v, o.term_col[2], r);
     return ok;
 }
 
@@ -646,24 +684,24 @@ VR_DEV bool op_raw(const OpDesc& o, const V& v, int64_t r, Contrib& x) {
             x.a = 1;
             return true;
         case OP_COUNT_VALID: {
-            bool ok = o.nterms > 0 ? terms_valid(o, v, r) : col_valid(v, o.col, r);
+            bool ok = o.nterms > 0 ? terms_valid(o, v, r) : in_valid(o, v, o.col, r);
             x.a = ok ? 1 : 0;
             return ok;
         }
         case OP_SUM_I32:
-            if (!col_valid(v, o.col, r)) return false;
+            if (!in_valid(o, v, o.col, r)) return false;
             x.a = (uint64_t)(int64_t)ld_i32(v, o.col, r);
             return true;
         case OP_SUM_I64:
-            if (!col_valid(v, o.col, r)) return false;
+            if (!in_valid(o, v, o.col, r)) return false;
             x.a = (uint64_t)ld_int(v, o.col, o.lane, r);
             return true;
         case OP_SUM_F64:
-            if (!col_valid(v, o.col, r)) return false;
+            if (!in_valid(o, v, o.col, r)) return false;
             x.a = (uint64_t)__double_as_longlong(ld_f64(v, o.col, r));
             return true;
         case OP_SUM_D128: {
-            if (!col_valid(v, o.col, r)) return false;
+            if (!in_valid(o, v, o.col, r)) return false;
             I128 d = ld_d128(v, o.col, r);
             x.a = d.lo;
             x.b = (uint64_t)d.hi;
@@ -674,36 +712,45 @@ VR_DEV bool op_raw(const OpDesc& o, const V& v, int64_t r, Contrib& x) {
                 x.h = 1;  // a null factor: the product is null
                 return true;
             }
-            I128 p = mul_i64(term_value(o, v, r, 0), term_value(o, v, r, 1));
-            bool fits = true;
+            // Fast path: every partial product fits int64 (mul.lo's sign
+            // extension equals mul.hi) and lies within the precision; other
+            // rows take the exact 128-bit path out of line.
+            const int64_t a = term_value(o, v, r, 0), b = term_value(o, v, r, 1);
+            int64_t p = a * b;
+            bool fits = __mul64hi(a, b) == (p >> 63);
+            int64_t c = 1;
             if (o.nterms == 3) {
-                I128 q;
-                fits = mul_i128_i64(p, term_value(o, v, r, 2), q);
+                c = term_value(o, v, r, 2);
+                const int64_t q = p * c;
+                fits = fits && __mul64hi(p, c) == (q >> 63);
                 p = q;
             }
-            if (!fits || !within_precision(p.lo, p.hi, o.prec)) {
-                // Spark's CheckOverflow on the product: null (non-ANSI) or an error (ANSI)
-                x.h = 1;
-                if (o.flags & OPF_CHECKED) x.g = 1;
+            if (fits && within_precision64(p, o.prec)) {
+                x.a = (uint64_t)p;
                 return true;
             }
-            if (p.hi == ((int64_t)p.lo >> 63)) {
-                x.a = p.lo;  // fits int64: the common case
+            const ProdResult s = product_exact(a, b, c, o.prec, (o.flags & OPF_CHECKED) != 0);
+            if (s.kind == ProdResult::kNull) {
+                // Spark's CheckOverflow on the product: null (non-ANSI) or an error (ANSI)
+                x.h = 1;
+                x.g = s.error;
+            } else if (s.kind == ProdResult::kInt64) {
+                x.a = s.lo;
             } else {
-                x.c = p.lo;
-                x.d = (uint64_t)p.hi;
+                x.c = s.lo;
+                x.d = s.hi;
                 x.e = 1;  // marks the 128-bit case in the raw form
             }
             return true;
         }
         case OP_MAX_KEY: {
-            if (!col_valid(v, o.col, r)) return false;
+            if (!in_valid(o, v, o.col, r)) return false;
             uint64_t k = o.lane == VR_FLOAT64 ? okey_f64(ld_f64(v, o.col, r)) : okey_i64(ld_int(v, o.col, o.lane, r));
             x.a = (o.flags & OPF_MIN) ? ~k : k;
             return true;
         }
         case OP_MAX_D128: {
-            if (!col_valid(v, o.col, r)) return false;
+            if (!in_valid(o, v, o.col, r)) return false;
             I128 d = ld_d128(v, o.col, r);
             uint64_t lo = d.lo, hi = (uint64_t)d.hi ^ 0x8000000000000000ull;
             if (o.flags & OPF_MIN) {
@@ -717,8 +764,8 @@ VR_DEV bool op_raw(const OpDesc& o, const V& v, int64_t r, Contrib& x) {
         case OP_MERGE_DSUM: {
             // WideDecimalSumMergeAgg.merge (VectorAggregates.scala:700-725): rows whose isEmpty is
             // null or true are skipped; a null sum on a non-empty row poisons the group.
-            if (!col_valid(v, o.col2, r) || bit_at(reinterpret_cast<const uint32_t*>(vdata(v, o.col2)), r)) return false;
-            if (!col_valid(v, o.col, r)) {
+            if (!in_valid(o, v, o.col2, r) || bit_at(reinterpret_cast<const uint32_t*>(vdata(v, o.col2)), r)) return false;
+            if (!in_valid(o, v, o.col, r)) {
                 x.e = kFlagNonEmpty | kFlagOverflow;
                 return true;
             }
@@ -731,8 +778,8 @@ VR_DEV bool op_raw(const OpDesc& o, const V& v, int64_t r, Contrib& x) {
         case OP_MERGE_DAVG: {
             // WideDecimalAvgMergeAgg.merge (VectorAggregates.scala:557-573): counts add when valid;
             // a null sum poisons the group.
-            if (col_valid(v, o.col2, r)) x.e = (uint64_t)ld_i64(v, o.col2, r);
-            if (!col_valid(v, o.col, r)) {
+            if (in_valid(o, v, o.col2, r)) x.e = (uint64_t)ld_i64(v, o.col2, r);
+            if (!in_valid(o, v, o.col, r)) {
                 x.g = kFlagOverflow;
                 return true;
             }

@@ -23,21 +23,11 @@
 #include "agg_device.cuh"
 #include "agg_kernels.cuh"
 
-namespace vr {
-
-}  // namespace vr
-
 #include "agg_main.cuh"
 
 namespace vr {
 
-template <int KW, int TIER>
-__global__ void __launch_bounds__(kMaxConsumerThreads + 32, 1) k_aggregate(const BatchDesc* __restrict__ descs,
-                                                                        const LaunchCfg cfg,
-                                                                        uint64_t* __restrict__ tile_counter) {
-    extern __shared__ __align__(128) unsigned char smem[];
-    aggregate_body<KW, TIER>(descs, cfg, tile_counter, smem);
-}
+SmemMap smem_map(int stages, int stage_bytes, int tier_bytes) { return smem_map_impl(stages, stage_bytes, tier_bytes); }
 
 // Deferred rows of one batch, against the HBM table only (rows are in batch
 // coordinates; the view is the batch's own columns).
@@ -432,53 +422,28 @@ __global__ void k_hash_rows(int nk, const vr_column_type* __restrict__ types, co
 }
 
 // ------------------------------------------------------------ launchers ---
-template <int KW, int TIER>
-static cudaError_t launch_agg_t(const BatchDesc* descs, const LaunchCfg& cfg, int blocks, uint64_t* tile_counter,
-                                cudaStream_t stream) {
-    auto fn = k_aggregate<KW, TIER>;
-    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, cfg.smem_bytes);
-    if (e != cudaSuccess) return e;
-    fn<<<blocks, cfg.consumer_threads + 32, cfg.smem_bytes, stream>>>(descs, cfg, tile_counter);
-    return cudaGetLastError();
-}
-
-template <int KW, int TIER>
-static int regs_t() {
-    cudaFuncAttributes a;
-    if (cudaFuncGetAttributes(&a, k_aggregate<KW, TIER>) != cudaSuccess) return 0;
-    return a.numRegs;
-}
-
+// The prebuilt aggregate kernels live in agg_aot_*.cu (one file per variant
+// so they compile in parallel). The direct tier never packs keys: one
+// variant serves every key width.
 int aggregate_kernel_regs(int kw, int tier) {
-    switch (kw * 2 + (tier == kTierDirect ? 0 : 1)) {
-        case 2: return regs_t<1, kTierDirect>();
-        case 3: return regs_t<1, kTierHash>();
-        case 4: return regs_t<2, kTierDirect>();
-        case 5: return regs_t<2, kTierHash>();
-        case 6: return regs_t<3, kTierDirect>();
-        case 7: return regs_t<3, kTierHash>();
-        case 8: return regs_t<4, kTierDirect>();
-        case 9: return regs_t<4, kTierHash>();
+    if (tier == kTierDirect) return aot_regs_direct();
+    switch (kw) {
+        case 1: return aot_regs_hash1();
+        case 2: return aot_regs_hash2();
+        case 3: return aot_regs_hash3();
+        case 4: return aot_regs_hash4();
     }
     return 0;
 }
 
 cudaError_t launch_aggregate(int kw, int tier, const BatchDesc* descs, const LaunchCfg& cfg, int blocks,
                              uint64_t* tile_counter, cudaStream_t stream) {
-    if (tier == kTierDirect) {
-        switch (kw) {
-            case 1: return launch_agg_t<1, kTierDirect>(descs, cfg, blocks, tile_counter, stream);
-            case 2: return launch_agg_t<2, kTierDirect>(descs, cfg, blocks, tile_counter, stream);
-            case 3: return launch_agg_t<3, kTierDirect>(descs, cfg, blocks, tile_counter, stream);
-            case 4: return launch_agg_t<4, kTierDirect>(descs, cfg, blocks, tile_counter, stream);
-        }
-    } else {
-        switch (kw) {
-            case 1: return launch_agg_t<1, kTierHash>(descs, cfg, blocks, tile_counter, stream);
-            case 2: return launch_agg_t<2, kTierHash>(descs, cfg, blocks, tile_counter, stream);
-            case 3: return launch_agg_t<3, kTierHash>(descs, cfg, blocks, tile_counter, stream);
-            case 4: return launch_agg_t<4, kTierHash>(descs, cfg, blocks, tile_counter, stream);
-        }
+    if (tier == kTierDirect) return aot_launch_direct(descs, cfg, blocks, tile_counter, stream);
+    switch (kw) {
+        case 1: return aot_launch_hash1(descs, cfg, blocks, tile_counter, stream);
+        case 2: return aot_launch_hash2(descs, cfg, blocks, tile_counter, stream);
+        case 3: return aot_launch_hash3(descs, cfg, blocks, tile_counter, stream);
+        case 4: return aot_launch_hash4(descs, cfg, blocks, tile_counter, stream);
     }
     return cudaErrorInvalidValue;
 }

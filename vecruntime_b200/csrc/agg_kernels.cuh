@@ -8,6 +8,18 @@
 
 namespace vr {
 
+// Prebuilt aggregate kernel variants (agg_aot_*.cu).
+#define VR_AOT_DECL(name)                                                                                     \
+    cudaError_t aot_launch_##name(const BatchDesc* descs, const LaunchCfg& cfg, int blocks, uint64_t* tile_counter, \
+                                  cudaStream_t stream);                                                      \
+    int aot_regs_##name();
+VR_AOT_DECL(direct)
+VR_AOT_DECL(hash1)
+VR_AOT_DECL(hash2)
+VR_AOT_DECL(hash3)
+VR_AOT_DECL(hash4)
+#undef VR_AOT_DECL
+
 SmemMap smem_map(int stages, int stage_bytes, int tier_bytes);
 
 // Launchers (all asynchronous on `stream`). `descs` lives in device memory.

@@ -32,7 +32,6 @@ __host__ __device__ inline SmemMap smem_map_impl(int stages, int stage_bytes, in
     m.total = m.tier + tier_bytes;
     return m;
 }
-SmemMap smem_map(int stages, int stage_bytes, int tier_bytes) { return smem_map_impl(stages, stage_bytes, tier_bytes); }
 
 VR_DEV void consumer_bar(int nt) { asm volatile("bar.sync 1, %0;" ::"r"(nt) : "memory"); }
 
@@ -424,8 +423,16 @@ VR_DEV void zero_words(uint64_t* p, int64_t n, int tid, int nt) {
 // (row base + j * NT + ctid for j < R). The host sizes direct-tier tiles to
 // exactly NT * R rows, so a full tile is one chunk with every lane busy.
 template <int KW, int TIER, int R>
-VR_DEV void consume_tile(const Program& P, const BatchDesc& D, const LaunchCfg& cfg, const TileView& v, int rows,
+VR_DEV void consume_tile(const Program& P, const BatchDesc& D, const LaunchCfg& cfg, const TileView& view, int rows,
                          int64_t row0, uint64_t* tier, int sslots, int NT, int ctid, uint32_t& new_groups) {
+#ifdef VR_JIT
+    // A register copy of the tile's column pointers: the per-spec kernel
+    // names every column by a constant, so only the ones it reads stay live,
+    // and stores to the accumulators cannot force them to be re-read.
+    const TileView v = view;
+#else
+    const TileView& v = view;
+#endif
     if (TIER == kTierDirect) {
         for (int base = 0; base < rows; base += R * NT) {
             int64_t r[R];
@@ -526,11 +533,14 @@ VR_DEV void aggregate_body(const BatchDesc* __restrict__ descs, const LaunchCfg&
 #ifdef VR_JIT
         consume_tile<KW, TIER, VR_JIT_RCHUNK>(P, D, cfg, v, h.rows, h.row0, tier, sslots, NT, ctid, new_groups);
 #else
-        switch (cfg.rchunk) {  // uniform
-            case 8: consume_tile<KW, TIER, 8>(P, D, cfg, v, h.rows, h.row0, tier, sslots, NT, ctid, new_groups); break;
-            case 2: consume_tile<KW, TIER, 2>(P, D, cfg, v, h.rows, h.row0, tier, sslots, NT, ctid, new_groups); break;
-            default: consume_tile<KW, TIER, 4>(P, D, cfg, v, h.rows, h.row0, tier, sslots, NT, ctid, new_groups);
-        }
+        // uniform; the host picks 8 for direct-tier tiles only
+        if (TIER == kTierDirect && cfg.rchunk == 8)
+            consume_tile<KW, TIER, TIER == kTierDirect ? 8 : 4>(P, D, cfg, v, h.rows, h.row0, tier, sslots, NT, ctid,
+                                                               new_groups);
+        else if (cfg.rchunk == 2)
+            consume_tile<KW, TIER, 2>(P, D, cfg, v, h.rows, h.row0, tier, sslots, NT, ctid, new_groups);
+        else
+            consume_tile<KW, TIER, 4>(P, D, cfg, v, h.rows, h.row0, tier, sslots, NT, ctid, new_groups);
 #endif
         __syncwarp();
         if ((ctid & 31) == 0) mbar_arrive(&empty[s]);

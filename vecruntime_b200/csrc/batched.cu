@@ -119,6 +119,11 @@ int vr_batched_create(const vr_batched_plan* plan, vr_batched** out) {
             set_thread_error("batched instances need live handles and device-resident batches");
             return VR_ERR_INVALID;
         }
+        if (const char* why = batch_nullability_error(h, bt)) {
+            delete b;
+            set_thread_error(why);
+            return VR_ERR_INVALID;
+        }
         if (h->device != b->device || std::memcmp(&h->plan.prog, &h0->plan.prog, sizeof(Program)) != 0 ||
             h->cfg.tier != h0->cfg.tier || h->cfg.tile_rows != h0->cfg.tile_rows || h->cfg.stages != h0->cfg.stages ||
             h->cfg.threads != h0->cfg.threads) {

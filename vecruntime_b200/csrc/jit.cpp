@@ -214,7 +214,9 @@ uint64_t fnv64(const std::string& s) {
 std::mutex g_mu;
 std::map<std::pair<int, uint64_t>, JitKernel*> g_cache;  // (device, source hash)
 
-bool compile_cubin(const std::string& src, std::vector<char>& cubin, std::string* err) {
+// `verbose`: ptxas resource usage (registers, spills, local memory) is
+// returned in *err on success too.
+bool compile_cubin(const std::string& src, std::vector<char>& cubin, std::string* err, bool verbose = false) {
     Nvrtc& n = nvrtc();
     if (!n.ok) {
         *err = n.why;
@@ -229,8 +231,8 @@ bool compile_cubin(const std::string& src, std::vector<char>& cubin, std::string
     // -default-device: the ABI's host prototypes in vrgpu.h are declarations
     // only here (never defined or called)
     const char* opts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "-lineinfo", "-DVR_JIT=1", "-default-device",
-                          "--device-int128"};
-    nvrtcResult r = n.compile(prog, 6, opts);
+                          "--device-int128", "--ptxas-options=-v"};
+    nvrtcResult r = n.compile(prog, verbose ? 7 : 6, opts);
     if (r != NVRTC_SUCCESS) {
         size_t ls = 0;
         n.log_size(prog, &ls);
@@ -239,6 +241,13 @@ bool compile_cubin(const std::string& src, std::vector<char>& cubin, std::string
         *err = "NVRTC compile failed: " + log.substr(0, 2000);
         n.destroy(&prog);
         return false;
+    }
+    if (verbose) {
+        size_t ls = 0;
+        n.log_size(prog, &ls);
+        std::string log(ls, '\0');
+        if (ls) n.log(prog, &log[0]);
+        *err = log;
     }
     size_t cs = 0;
     n.cubin_size(prog, &cs);
@@ -276,7 +285,7 @@ static std::string jit_source(const Program& P, int kw, int tier, int rchunk) {
 
 bool jit_compile_only(const Program& P, int kw, int tier, int rchunk, size_t* cubin_bytes, std::string* err) {
     std::vector<char> cubin;
-    if (!compile_cubin(jit_source(P, kw, tier, rchunk), cubin, err)) return false;
+    if (!compile_cubin(jit_source(P, kw, tier, rchunk), cubin, err, true)) return false;
     if (cubin_bytes) *cubin_bytes = cubin.size();
     return true;
 }

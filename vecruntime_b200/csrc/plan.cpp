@@ -109,6 +109,13 @@ struct Builder {
             }
             if (!nullable) return 0;  // COUNT_ROWS is always op 0, word 0
         }
+        {
+            bool nullable = false;
+            for (int t = 0; t < nterms; ++t) nullable |= P.col_nullable[tc[t]] != 0;
+            if (scol >= 0) nullable |= P.col_nullable[scol] != 0;
+            if (scol2 >= 0) nullable |= P.col_nullable[scol2] != 0;
+            if (nullable) flags |= OPF_NULLABLE;
+        }
         int keyflags = flags | ((terms_fn ? terms_fn->product_precision : 0) << 8);
         auto key = std::make_tuple(kind, scol, scol2, keyflags, tc[0] * 4096 + tc[1] * 64 + tc[2], ts[0] * 9 + ts[1] * 3 + ts[2],
                                    nterms, ta[0], ta[1], ta[2]);

@@ -126,5 +126,7 @@ int agg_resolve_all(vr_agg* h);
 cudaError_t agg_launch(vr_agg* h, const BatchDesc* descs, const LaunchCfg& L, int blocks, uint64_t* tile_counter,
                        cudaStream_t st);
 int64_t tiles_for(const vr_agg* h, int64_t rows);
+// Why a batch breaks the spec's nullability (a bitmap on a non-nullable column), or null.
+const char* batch_nullability_error(const vr_agg* h, const vr_batch& b);
 void set_thread_error(const std::string& msg);
 }  // namespace vr

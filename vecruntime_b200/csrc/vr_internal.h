@@ -151,7 +151,10 @@ constexpr uint64_t kErrSpillFull = 8;
 constexpr uint64_t kErrBadKey = 16;     // dictionary id outside its declared range
 constexpr uint64_t kErrProduct = 32;    // ANSI: a decimal product reached its precision
 
-enum OpFlagsExtra : uint8_t { OPF_CHECKED = 2 };  // OP_SUM_PROD: product overflow is an error
+enum OpFlagsExtra : uint8_t {
+    OPF_CHECKED = 2,  // OP_SUM_PROD: product overflow is an error
+    OPF_NULLABLE = 4  // some input column of the op is declared nullable (else no validity test)
+};
 
 constexpr int kTierDirect = 0;
 constexpr int kTierHash = 1;
