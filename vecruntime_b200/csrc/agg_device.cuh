@@ -607,7 +607,7 @@ VR_DEV uint64_t* find_or_insert(uint64_t* table, int64_t mask, int sw, const uin
 // kind         global words                           private words
 // COUNT_*      a=count                                a=count
 // SUM_I32      a=sum                                  a=sum
-// SUM_I64      a=sum lo32 (u) b=sum hi32 (s)          a=int64 sum  b=wraps
+// SUM_I64      a=sum of lo32 (s) b=sum of hi32 (s)    a=int64 sum  b=wraps
 // SUM_F64      a=sum b=compensation                   a=sum b=compensation
 // SUM_D128     a..d=32-bit limbs (d signed)           a,b=int128 sum  c=wraps
 // SUM_PROD     a,b=cs  c..f=limbs  g=ANSI flag        a=int64 sum b=wraps c,d=int128 e=wraps
@@ -621,8 +621,15 @@ struct Contrib {
 };
 
 VR_DEV void czero(Contrib& x) { x.a = x.b = x.c = x.d = x.e = x.f = x.g = x.h = 0; }
-VR_DEV uint64_t lo32(int64_t x) { return (uint64_t)(uint32_t)x; }
 VR_DEV uint64_t hi32(int64_t x) { return (uint64_t)(int64_t)(int32_t)(x >> 32); }
+// Signed carry-save split of an int64: x = lo + hi * 2^32 with lo the
+// sign-extended low 32 bits, so |x| < 2^31 has hi == 0 (one atomic, not two).
+// Table words accumulate lo and hi parts; a low word's total is read signed.
+VR_DEV void split_cs(int64_t x, uint64_t& lo, uint64_t& hi) {
+    const int64_t l = (int64_t)(int32_t)x;
+    lo = (uint64_t)l;
+    hi = (uint64_t)((x >> 32) + (l < 0 ? 1 : 0));
+}
 
 // Validity of input column c of op o at row r: only columns the spec
 // declares nullable are tested (a non-nullable column never carries a bitmap).
@@ -805,12 +812,9 @@ template <int K>
 VR_DEV void raw_to_global(const OpDesc& o, Contrib& x) {
     (void)o;
     switch (K) {
-        case OP_SUM_I64: {
-            int64_t v = (int64_t)x.a;
-            x.a = lo32(v);
-            x.b = hi32(v);
+        case OP_SUM_I64:
+            split_cs((int64_t)x.a, x.a, x.b);
             break;
-        }
         case OP_SUM_D128:
             limbs_of(x.a, x.b, x.a, x.b, x.c, x.d);
             break;
@@ -820,9 +824,7 @@ VR_DEV void raw_to_global(const OpDesc& o, Contrib& x) {
                 x.a = x.b = 0;
                 limbs_of(lo, hi, x.c, x.d, x.e, x.f);
             } else {
-                int64_t v = (int64_t)x.a;
-                x.a = lo32(v);
-                x.b = hi32(v);
+                split_cs((int64_t)x.a, x.a, x.b);
             }
             break;
         case OP_MERGE_DSUM:
@@ -831,8 +833,7 @@ VR_DEV void raw_to_global(const OpDesc& o, Contrib& x) {
         case OP_MERGE_DAVG: {
             int64_t n = (int64_t)x.e;
             limbs_of(x.a, x.b, x.a, x.b, x.c, x.d);
-            x.e = lo32(n);
-            x.f = hi32(n);
+            split_cs(n, x.e, x.f);
             break;
         }
         default:

@@ -115,8 +115,8 @@ VR_DEV Wide op_total(uint8_t op, const uint64_t* w, bool& overflow_flag) {
         case OP_SUM_I32:
             wide_add_shifted(t, w[0], true, 0);
             break;
-        case OP_SUM_I64:
-            wide_add_shifted(t, w[0], false, 0);
+        case OP_SUM_I64:  // low word: signed (a sum of signed or unsigned 32-bit parts)
+            wide_add_shifted(t, w[0], true, 0);
             wide_add_shifted(t, w[1], true, 1);
             break;
         case OP_SUM_D128:
@@ -128,7 +128,7 @@ VR_DEV Wide op_total(uint8_t op, const uint64_t* w, bool& overflow_flag) {
             wide_add_shifted(t, w[3], true, 3);
             break;
         case OP_SUM_PROD:
-            wide_add_shifted(t, w[0], false, 0);
+            wide_add_shifted(t, w[0], true, 0);
             wide_add_shifted(t, w[1], true, 1);
             wide_add_shifted(t, w[2], false, 0);
             wide_add_shifted(t, w[3], false, 1);

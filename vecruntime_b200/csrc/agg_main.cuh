@@ -533,10 +533,11 @@ VR_DEV void aggregate_body(const BatchDesc* __restrict__ descs, const LaunchCfg&
 #ifdef VR_JIT
         consume_tile<KW, TIER, VR_JIT_RCHUNK>(P, D, cfg, v, h.rows, h.row0, tier, sslots, NT, ctid, new_groups);
 #else
-        // uniform; the host picks 8 for direct-tier tiles only
-        if (TIER == kTierDirect && cfg.rchunk == 8)
-            consume_tile<KW, TIER, TIER == kTierDirect ? 8 : 4>(P, D, cfg, v, h.rows, h.row0, tier, sslots, NT, ctid,
-                                                               new_groups);
+        // uniform: the host picks 2, 4 or 8 for direct-tier tiles, 1 for the hash tier
+        if (TIER != kTierDirect)
+            consume_tile<KW, TIER, 1>(P, D, cfg, v, h.rows, h.row0, tier, sslots, NT, ctid, new_groups);
+        else if (cfg.rchunk == 8)
+            consume_tile<KW, TIER, 8>(P, D, cfg, v, h.rows, h.row0, tier, sslots, NT, ctid, new_groups);
         else if (cfg.rchunk == 2)
             consume_tile<KW, TIER, 2>(P, D, cfg, v, h.rows, h.row0, tier, sslots, NT, ctid, new_groups);
         else

@@ -24,7 +24,7 @@ struct LaunchCfg {
     int32_t s_probes;          // shared-memory cache probe limit
     int32_t smem_bytes;        // dynamic shared memory of the launch
     int32_t tier_bytes;        // shared memory of the tier area
-    int32_t rchunk;            // rows per consumer thread per chunk: 2, 4 or 8
+    int32_t rchunk;            // rows per consumer thread per chunk: 2, 4 or 8 (direct), 1 (hash)
     int32_t pad;
     StageLayout lay;
 };

@@ -145,7 +145,9 @@ int vr_batched_create(const vr_batched_plan* plan, vr_batched** out) {
     b->cfg.tier_bytes = max_tier_bytes;
     b->cfg.smem_bytes = smem_map(b->cfg.stages, b->cfg.lay.stage_bytes, max_tier_bytes).total;
     const DeviceInfo& di = device_info(b->device);
-    b->blocks = di.sms * ((2 * b->cfg.smem_bytes <= di.smem_optin) ? 2 : 1);
+    // the first instance's kernel serves all: its CTAs per SM, if the
+    // batch's (largest) shared-memory footprint still allows them
+    b->blocks = std::min(h0->blocks, di.sms * (di.fits(2, b->cfg.smem_bytes) ? 2 : 1));
     // descriptors: instance i's tiles follow instance i-1's
     std::vector<ZeroSpan> spans;
     int64_t tile = 0;

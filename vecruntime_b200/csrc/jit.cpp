@@ -264,17 +264,18 @@ bool jit_enabled() {
     return !(e && std::strcmp(e, "0") == 0);
 }
 
-static std::string jit_source(const Program& P, int kw, int tier, int rchunk) {
+static std::string jit_source(const Program& P, const JitShape& S) {
     std::string src = kPrelude;
-    src += "#define VR_JIT_KW " + std::to_string(kw) + "\n#define VR_JIT_TIER " + std::to_string(tier) + "\n";
-    src += "#define VR_JIT_RCHUNK " + std::to_string(rchunk) + "\n";
+    src += "#define VR_JIT_KW " + std::to_string(S.kw) + "\n#define VR_JIT_TIER " + std::to_string(S.tier) + "\n";
+    src += "#define VR_JIT_RCHUNK " + std::to_string(S.rchunk) + "\n";
     src += "#define VR_JIT_NUM_OPS " + std::to_string(P.num_ops) + "\n";
     src += "#include \"agg_device.cuh\"\nnamespace vr {\n__constant__ const Program kJitProg = ";
     src += program_literal(P);
     src += ";\n}\n#include \"agg_main.cuh\"\n";
     src += hooks(P);
     src +=
-        "extern \"C\" __global__ void __launch_bounds__(vr::kMaxConsumerThreads + 32, 1)\n"
+        "extern \"C\" __global__ void __launch_bounds__(" + std::to_string(S.threads + 32) + ", " +
+        std::to_string(S.min_blocks) + ")\n"
         "vr_jit_aggregate(const vr::BatchDesc* __restrict__ descs, const vr::LaunchCfg cfg,\n"
         "                 unsigned long long* __restrict__ tile_counter) {\n"
         "    extern __shared__ __align__(128) unsigned char smem[];\n"
@@ -283,15 +284,15 @@ static std::string jit_source(const Program& P, int kw, int tier, int rchunk) {
     return src;
 }
 
-bool jit_compile_only(const Program& P, int kw, int tier, int rchunk, size_t* cubin_bytes, std::string* err) {
+bool jit_compile_only(const Program& P, const JitShape& S, size_t* cubin_bytes, std::string* err) {
     std::vector<char> cubin;
-    if (!compile_cubin(jit_source(P, kw, tier, rchunk), cubin, err, true)) return false;
+    if (!compile_cubin(jit_source(P, S), cubin, err, true)) return false;
     if (cubin_bytes) *cubin_bytes = cubin.size();
     return true;
 }
 
-JitKernel* jit_get(const Program& P, int kw, int tier, int rchunk, int device, std::string* err) {
-    std::string src = jit_source(P, kw, tier, rchunk);
+JitKernel* jit_get(const Program& P, const JitShape& S, int device, std::string* err) {
+    std::string src = jit_source(P, S);
     uint64_t h = fnv64(src);
     for (int i = 0; i < jitsrc::kNum; ++i) h ^= fnv64(jitsrc::kTexts[i]) * (i + 3);
     std::lock_guard<std::mutex> lk(g_mu);

@@ -59,8 +59,12 @@ struct JitKernel;
 
 struct DeviceInfo {
     int sms = 148;
-    int smem_optin = 232448;
+    int smem_optin = 232448;     // per block
+    int smem_per_sm = 233472;
+    int smem_reserved = 1024;    // per block, by the system
     bool ready = false;
+    // Whether `blocks` CTAs of `smem` dynamic shared bytes fit on one SM.
+    bool fits(int blocks, int smem) const { return blocks * (smem + smem_reserved) <= smem_per_sm; }
 };
 DeviceInfo& device_info(int device);
 
