@@ -1,0 +1,122 @@
+"""GPU parity of the batched and serving entry points.
+
+Batched: many uneven instances (rows 2^8..2^14, cardinality 1..2^12) in one
+persistent launch, with and without CUDA-graph replay, and one launch per
+instance; every instance's groups must equal the oracle's, on the first run
+and on a replay (the run resets the tables).
+
+Serving: several live queries whose requests arrive interleaved; each
+query's result must equal the oracle's and the same query run alone."""
+import numpy as np
+import pytest
+
+import vecruntime_b200 as vr
+from vecruntime_b200 import aggregate as A
+from vecruntime_b200 import columns as Cc
+from vecruntime_b200 import datagen as G
+from vecruntime_b200 import native as N
+
+from oracle.pyoracle import ORC_FP_COMPENSATED, Oracle
+from parity import compare
+
+pytestmark = pytest.mark.gpu
+
+
+def oracle_of(w, batches):
+    o = Oracle(w.spec())
+    for b in batches:
+        o.update(b)
+    return o.output_types, o.emit(ORC_FP_COMPENSATED), o.num_groups()
+
+
+def shared_choice():
+    """One launch configuration for every instance (a batched launch needs it)."""
+    t = N.TuneChoice()
+    t.tier = 1
+    t.threads = 256
+    t.tile_rows = 1024
+    t.smem_slots = 256
+    return t
+
+
+@pytest.mark.parametrize("mode,use_graph", [(N.VR_BATCHED_PERSISTENT, False), (N.VR_BATCHED_PERSISTENT, True),
+                                            (N.VR_BATCHED_PLAIN, False)])
+def test_batched_instances_match_the_oracle(cuda, mode, use_graph):
+    ws = G.batched_instances(n=24, max_log_rows=14, max_log_card=12)
+    aggs, dbs, keep = [], [], []
+    for w in ws:
+        aggs.append(vr.GpuHashAggregate(w.columns, w.keys, w.functions, est_groups=w.est_groups,
+                                        max_batch_rows=w.rows, tune=shared_choice()))
+        db, t = Cc.to_device(w.batch())
+        dbs.append(db)
+        keep.append(t)
+    b = vr.GpuBatchedAggregate(aggs, dbs, mode=mode, use_graph=use_graph)
+    try:
+        for run in range(2):  # the second run replays (graph) and must reset the tables
+            b.run()
+            for w, a in zip(ws, aggs):
+                n = a.num_groups()
+                compare(w.spec(), a.output_types, a.emit(), n, *oracle_of(w, [w.batch()]))
+    finally:
+        b.close()
+        for a in aggs:
+            a.close()
+
+
+def test_batched_refuses_mixed_launch_shapes(cuda):
+    ws = G.batched_instances(n=2, max_log_rows=12, max_log_card=4)
+    other = shared_choice()
+    other.tile_rows = 512
+    aggs = [vr.GpuHashAggregate(ws[0].columns, ws[0].keys, ws[0].functions, max_batch_rows=ws[0].rows,
+                                tune=shared_choice()),
+            vr.GpuHashAggregate(ws[1].columns, ws[1].keys, ws[1].functions, max_batch_rows=ws[1].rows, tune=other)]
+    dbs, keep = [], []
+    for w in ws:
+        db, t = Cc.to_device(w.batch())
+        dbs.append(db)
+        keep.append(t)
+    with pytest.raises(vr.VrError):
+        vr.GpuBatchedAggregate(aggs, dbs)
+    for a in aggs:
+        a.close()
+
+
+def test_serving_mix_equals_alone_and_the_oracle(cuda):
+    rng = np.random.default_rng(77)
+    queries = []
+    for q, (card, rows) in enumerate([(50, 40_000), (5_000, 60_000), (300_000, 50_000)]):
+        domain = rng.integers(-(1 << 62), 1 << 62, size=card, dtype=np.int64)
+        k = domain[rng.integers(0, card, size=rows)]
+        v1 = rng.integers(-10**6, 10**6, size=rows, dtype=np.int64)
+        v2 = rng.standard_normal(rows)
+        nulls = rng.random(rows) < 0.05
+        cols = [Cc.longs(k, nullable=False), Cc.longs(v1, nulls, nullable=True), Cc.doubles(v2, nullable=False)]
+        w = G.Workload(f"q{q}", cols, [0], [A.CountAgg(), A.CountAgg(1), A.SumLongAgg(1), A.MinMaxAgg(1, True),
+                                           A.MinMaxAgg(1, False), A.SumDoubleAgg(2)], card, rows)
+        chunks = [w.batch(lo, min(rows, lo + 8192)) for lo in range(0, rows, 8192)]
+        queries.append((w, chunks))
+    srv = vr.AggregateServer(slots=4, hbm_cap_bytes=8 << 30)
+    try:
+        qids = [srv.open_query(w.columns, w.keys, w.functions, est_groups=w.est_groups, max_batch_rows=8192)
+                for w, _ in queries]
+        tickets = []
+        longest = max(len(c) for _, c in queries)
+        for i in range(longest):  # interleaved arrivals
+            for qid, (w, chunks) in zip(qids, queries):
+                if i < len(chunks):
+                    tickets.append(srv.submit(qid, chunks[i]))
+        lat = [srv.wait(t) for t in tickets]
+        assert all(x >= 0 for x in lat)
+        for qid, (w, chunks) in zip(qids, queries):
+            types, arrays, n = srv.results(qid)
+            want = oracle_of(w, chunks)
+            compare(w.spec(), types, arrays, n, *want)
+            alone = vr.GpuHashAggregate(w.columns, w.keys, w.functions, est_groups=w.est_groups, max_batch_rows=8192)
+            for c in chunks:
+                alone.consume(c)
+            compare(w.spec(), types, arrays, n, alone.output_types, alone.emit(), alone.num_groups())
+            alone.close()
+        st = srv.stats()
+        assert st.completed == len(tickets) and st.rejected == 0
+    finally:
+        srv.close()

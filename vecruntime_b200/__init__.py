@@ -5,16 +5,16 @@ kernels; this package is its Python host mirror of the reference's operator
 interface. Importing it does not touch the GPU; creating an aggregate loads
 the library and fails loudly when it was not built.
 """
-from .aggregate import (AggFunction, AverageAgg, AverageMergeAgg, CountAgg, CountMergeAgg, DecimalProduct,
-                        GpuHashAggregate, MinMaxAgg, Spec, SumDoubleAgg, SumLongAgg, WideDecimalAvgAgg,
+from .aggregate import (AggFunction, AggregateServer, AverageAgg, AverageMergeAgg, CountAgg, CountMergeAgg,
+                        DecimalProduct, GpuBatchedAggregate, GpuHashAggregate, MinMaxAgg, Spec, SumDoubleAgg, SumLongAgg, WideDecimalAvgAgg,
                         WideDecimalAvgMergeAgg, WideDecimalSumAgg, WideDecimalSumMergeAgg)
 from .columns import (Col, DeviceBatch, HostBatch, bools, decimals, decimals128, dict_ids, doubles, host_batch,
                       ints, longs, pack_bits, unpack_bits)
 from .native import VrError, lib
 
 __all__ = [
-    "AggFunction", "AverageAgg", "AverageMergeAgg", "CountAgg", "CountMergeAgg", "DecimalProduct",
-    "GpuHashAggregate", "MinMaxAgg", "Spec", "SumDoubleAgg", "SumLongAgg", "WideDecimalAvgAgg",
+    "AggFunction", "AggregateServer", "AverageAgg", "AverageMergeAgg", "CountAgg", "CountMergeAgg", "DecimalProduct",
+    "GpuBatchedAggregate", "GpuHashAggregate", "MinMaxAgg", "Spec", "SumDoubleAgg", "SumLongAgg", "WideDecimalAvgAgg",
     "WideDecimalAvgMergeAgg", "WideDecimalSumAgg", "WideDecimalSumMergeAgg", "Col", "DeviceBatch", "HostBatch",
     "bools", "decimals", "decimals128", "dict_ids", "doubles", "host_batch", "ints", "longs", "pack_bits",
     "unpack_bits", "VrError", "lib",

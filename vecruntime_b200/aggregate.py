@@ -239,3 +239,130 @@ class GpuHashAggregate:
             self.close()
         except Exception:
             pass
+
+
+# ------------------------------------------------------------------ batched
+class GpuBatchedAggregate:
+    """Many independent aggregates (one Spark task's batch each) run by one
+    persistent launch (mode VR_BATCHED_PERSISTENT, optionally replayed from a
+    CUDA graph) or by one launch per instance (VR_BATCHED_PLAIN). The
+    instances must share one spec shape and one launch configuration: create
+    them with the same `tune` choice. No reference counterpart: the reference
+    runs one task per thread (VectorHashAggregateExec.scala:248-302)."""
+
+    def __init__(self, instances: Sequence["GpuHashAggregate"], device_batches: Sequence, mode: int = 0,
+                 use_graph: bool = False):
+        self._lib = N.lib()
+        self.instances = list(instances)
+        self._batches = list(device_batches)
+        self._hs = (C.c_void_p * len(self.instances))(*[a.h.value for a in self.instances])
+        self._bs = (N.Batch * len(self._batches))(*[b.ctypes() for b in self._batches])
+        plan = N.BatchedPlan(len(self.instances), self._hs, self._bs, mode, 1 if use_graph else 0)
+        h = C.c_void_p()
+        rc = self._lib.vr_batched_create(C.byref(plan), C.byref(h))
+        if rc:
+            raise N.VrError(rc, "vr_batched_create: " + (self._lib.vr_thread_last_error() or b"").decode())
+        self.h = h
+
+    def run(self, stream: int = 0) -> None:
+        """Resets every instance's table and aggregates every instance's batch,
+        asynchronously on `stream` (0: the first instance's stream)."""
+        rc = self._lib.vr_batched_run(self.h, C.c_void_p(stream) if stream else None)
+        if rc:
+            raise N.VrError(rc, "vr_batched_run: " + (self._lib.vr_thread_last_error() or b"").decode())
+
+    def close(self) -> None:
+        if self.h:
+            self._lib.vr_batched_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------------------ serving
+class AggregateServer:
+    """Continuous batching of partial-aggregation requests over resident
+    per-query tables (vr_srv_*): requests from many tasks are admitted as soon
+    as a device slot and the HBM budget allow; latency is submit -> device
+    completion. No reference counterpart."""
+
+    def __init__(self, device: int = 0, slots: int = 8, hbm_cap_bytes: int = 120 << 30,
+                 staging_bytes_per_slot: int = 0):
+        self._lib = N.lib()
+        cfg = N.SrvConfig(device, slots, hbm_cap_bytes, staging_bytes_per_slot, 0, 0)
+        h = C.c_void_p()
+        rc = self._lib.vr_srv_create(C.byref(cfg), C.byref(h))
+        if rc:
+            raise N.VrError(rc, "vr_srv_create: " + (self._lib.vr_thread_last_error() or b"").decode())
+        self.h = h
+        self._specs = {}
+        self._pending = {}  # ticket -> batch kept alive until it completes
+
+    def _check(self, rc, what):
+        if rc:
+            raise N.VrError(rc, f"{what}: " + (self._lib.vr_thread_last_error() or b"").decode())
+
+    def open_query(self, columns, keys, functions, est_groups: int = 0, max_batch_rows: int = 0) -> int:
+        spec = Spec(columns, keys, functions, est_groups, max_batch_rows)
+        q = C.c_int32()
+        self._check(self._lib.vr_srv_open_query(self.h, C.byref(spec.spec), C.byref(q)), "vr_srv_open_query")
+        self._specs[q.value] = spec
+        return q.value
+
+    def submit(self, query: int, batch) -> int:
+        cb = batch.ctypes()
+        t = C.c_uint64()
+        self._check(self._lib.vr_srv_submit(self.h, query, C.byref(cb), C.byref(t)), "vr_srv_submit")
+        self._pending[t.value] = (batch, cb)
+        return t.value
+
+    def wait(self, ticket: int) -> float:
+        ms = C.c_double()
+        self._check(self._lib.vr_srv_wait(self.h, ticket, C.byref(ms)), "vr_srv_wait")
+        self._pending.pop(ticket, None)
+        return ms.value
+
+    def drain(self) -> None:
+        self._check(self._lib.vr_srv_drain(self.h), "vr_srv_drain")
+        self._pending.clear()
+
+    def results(self, query: int):
+        """(output types, arrays, group count) of a query after its queued requests."""
+        h = C.c_void_p()
+        self._check(self._lib.vr_srv_query_handle(self.h, query, C.byref(h)), "vr_srv_query_handle")
+        n = C.c_int32()
+        types = (N.ColumnType * 64)()
+        N.check(self._lib.vr_agg_output_schema(h, C.byref(n), types, 64), "output schema")
+        out_types = [types[i] for i in range(n.value)]
+        g = C.c_int64()
+        N.check(self._lib.vr_agg_num_groups(h, C.byref(g)), "vr_agg_num_groups")
+        arrays = [_out_arrays(t, g.value) for t in out_types]
+        outs = (N.OutColumn * max(1, len(arrays)))()
+        for i, (d, v) in enumerate(arrays):
+            outs[i].data = d.ctypes.data
+            outs[i].validity = v.ctypes.data
+        N.check(self._lib.vr_agg_emit(h, 0, g.value, outs, N.VR_HOST), "vr_agg_emit")
+        return out_types, arrays, g.value
+
+    def close_query(self, query: int) -> None:
+        self._check(self._lib.vr_srv_close_query(self.h, query), "vr_srv_close_query")
+
+    def stats(self) -> N.SrvStats:
+        st = N.SrvStats()
+        self._lib.vr_srv_get_stats(self.h, C.byref(st))
+        return st
+
+    def close(self) -> None:
+        if self.h:
+            self._lib.vr_srv_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
