@@ -371,6 +371,167 @@ def run_e2e(args, w, lib, device, out_types):
             "d2h_bytes_per_step": d2h, "ms_per_step": ms, "chunk_rows": chunk}
 
 
+# ------------------------------------------------------------------ batched (C4)
+def batched_choice():
+    """The one launch configuration every instance of a batched launch shares:
+    the hash tier's two-CTAs-per-SM shape (1024-row tiles, 256 consumer
+    threads, a 256-slot shared hot-key cache in front of each instance's HBM
+    table), the best measured on the high-cardinality shape."""
+    from vecruntime_b200 import native as N
+
+    t = N.TuneChoice()
+    t.tier, t.threads, t.tile_rows, t.smem_slots = 1, 256, 1024, 256
+    return t
+
+
+def run_batched(args, device):
+    """512 uneven instances (rows log-uniform 2^10..2^22, cardinality
+    log-uniform 1..2^20): one persistent launch replayed from a CUDA graph,
+    against one launch per instance. A step resets every table and
+    aggregates every instance's device-resident batch."""
+    import torch
+
+    import vecruntime_b200 as vr
+    from vecruntime_b200 import columns as Cc
+    from vecruntime_b200 import datagen as G
+    from vecruntime_b200 import native as N
+
+    torch.cuda.set_device(device)
+    ws = G.batched_instances(n=args.instances)
+    log(f"[batched] {len(ws)} instances, {sum(w.rows for w in ws)} rows")
+    aggs, dbs, keep = [], [], []
+    for w in ws:
+        aggs.append(vr.GpuHashAggregate(w.columns, w.keys, w.functions, est_groups=w.est_groups,
+                                        max_batch_rows=w.rows, device=device, tune=batched_choice()))
+        db, t = Cc.to_device(w.batch(), device)
+        dbs.append(db)
+        keep.append(t)
+    stream = torch.cuda.Stream(device=device)
+    rows = sum(w.rows for w in ws)
+    in_bytes = sum(G.input_bytes(w) for w in ws)
+
+    def timed(b):
+        for _ in range(args.warmup):
+            b.run(stream.cuda_stream)
+        ms = []
+        for _ in range(args.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            b.run(stream.cuda_stream)
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return float(np.mean(ms))
+
+    torch.cuda.synchronize(device)
+    with ClockSampler(device) as clocks:
+        persistent = vr.GpuBatchedAggregate(aggs, dbs, mode=N.VR_BATCHED_PERSISTENT, use_graph=True)
+        ms_p = timed(persistent)
+        persistent.close()
+        plain = vr.GpuBatchedAggregate(aggs, dbs, mode=N.VR_BATCHED_PLAIN)
+        ms_l = timed(plain)
+        plain.close()
+    launches = 3  # zero, aggregate, status gather
+    peak, peak_kind = measured_peaks()
+    for a in aggs:
+        a.close()
+    return {
+        "metric": METRIC, "value": rows / (ms_p * 1e-3), "unit": "rows/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_p, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int64/f64", "data": "synthetic (seeded; shapes of the workload, no benchmark data reproduced)",
+        "config": {"workload": f"batched uneven instances: {len(ws)} aggregates, {rows} rows, rows log-uniform "
+                               "2^10..2^22, cardinality log-uniform 1..2^20, int64 key, int64 + float64 values, "
+                               "count/sum/min/max", "mode": "one persistent launch replayed from a CUDA graph",
+                   "l2": "inputs larger than L2 (%.2f GB)" % (in_bytes / 1e9)},
+        "roofline": {"bound": "hbm", "achieved": in_bytes / (ms_p * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": in_bytes / (ms_p * 1e-3) / 1e9 / peak, "peak_kind": peak_kind, "traffic": None,
+                     "algorithmic_bytes_per_launch": in_bytes, "kernel_ms": ms_p},
+        "one_launch_per_instance": {"value": rows / (ms_l * 1e-3), "unit": "rows/s", "ms_per_step": ms_l},
+        "speedup_vs_one_launch_per_instance": ms_l / ms_p,
+        "gpu_launches": launches * args.steps,
+        "clocks": clocks.summary(),
+    }
+
+
+# ------------------------------------------------------------------ serving (C5)
+def run_serving(args, device):
+    """16 live queries (resident tables of 1e3..1e7 groups) fed by Poisson
+    arrivals (args.rate requests/s in total) of batches with log-uniform
+    4,096..1,048,576 rows, for args.seconds: p50/p99 latency (submit ->
+    device completion) and rows/s. Request batches come from a pinned pool
+    (4 per query) reused by the seeded trace."""
+    import threading as th
+
+    import torch
+
+    import vecruntime_b200 as vr
+    from vecruntime_b200 import aggregate as A
+    from vecruntime_b200 import columns as Cc
+    from vecruntime_b200 import datagen as G
+    from vecruntime_b200 import native as N
+
+    torch.cuda.set_device(device)
+    lib = N.lib()
+    rng = np.random.default_rng(G.SEEDS["serving"])
+    fns = [A.CountAgg(), A.SumLongAgg(1), A.MinMaxAgg(1, True), A.MinMaxAgg(1, False), A.SumDoubleAgg(2),
+           A.MinMaxAgg(2, True), A.MinMaxAgg(2, False)]
+    srv = vr.AggregateServer(device=device, slots=8, hbm_cap_bytes=120 << 30)
+    queries, pool, bufs = [], [], []
+    max_rows = 1 << 20
+    for q in range(16):
+        card = int(round(10 ** rng.uniform(3, 7)))
+        domain = rng.integers(-(1 << 62), 1 << 62, size=card, dtype=np.int64)
+        batches = []
+        for _ in range(4):
+            n = int(round(2 ** rng.uniform(12, 20)))
+            cols = [Cc.longs(domain[rng.integers(0, card, size=n)], nullable=False),
+                    Cc.longs(rng.integers(-10**6, 10**6, size=n, dtype=np.int64), nullable=False),
+                    Cc.doubles(rng.standard_normal(n), nullable=False)]
+            w = G.Workload(f"q{q}", cols, [0], fns, card, n)
+            pcols, pb = pinned_copy(w, lib)
+            bufs += pb
+            batches.append(Cc.HostBatch(pcols, n))
+        qid = srv.open_query(cols, [0], fns, est_groups=card, max_batch_rows=max_rows)
+        queries.append(qid)
+        pool.append(batches)
+    # the seeded trace: arrival times and (query, batch) picks
+    n_req = int(args.rate * args.seconds)
+    gaps = rng.exponential(1.0 / args.rate, size=n_req)
+    picks = [(int(rng.integers(0, 16)), int(rng.integers(0, 4))) for _ in range(n_req)]
+    tickets, rows_done = [], 0
+    with ClockSampler(device) as clocks:
+        t0 = time.perf_counter()
+        due = t0
+        for gap, (q, b) in zip(gaps, picks):
+            due += gap
+            d = due - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            tickets.append(srv.submit(queries[q], pool[q][b]))
+            rows_done += pool[q][b].num_rows
+        lat = [srv.wait(t) for t in tickets]
+        wall = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    for p in bufs:
+        lib.vr_host_free(p)
+    lat = np.array(lat)
+    return {
+        "metric": METRIC, "value": rows_done / wall, "unit": "rows/s", "n_gpus": 1, "steps": n_req,
+        "warmup": 0, "ms_per_step": float(np.mean(lat)), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int64/f64", "data": "synthetic (seeded trace; no benchmark data reproduced)",
+        "config": {"workload": f"serving loop: 16 live queries (1e3..1e7 groups), Poisson arrivals at "
+                               f"{args.rate:g} requests/s for {args.seconds:g} s, batches of 4,096..1,048,576 "
+                               "rows from pinned host memory", "hbm_cap_gb": 120},
+        "serving": {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                    "max_ms": float(lat.max()), "requests": n_req, "admitted_immediately": st.admitted_immediately,
+                    "queued": st.queued, "rejected": st.rejected, "hbm_peak_gb": st.hbm_peak / 1e9,
+                    "offered_rows_per_s": rows_done / float(np.sum(gaps))},
+        "gpu_launches": int(st.completed),
+        "clocks": clocks.summary(),
+    }
+
+
 # ------------------------------------------------------------------ reference arm
 def run_reference(args):
     """The CPU port of the reference's aggregate (oracle/) on the host cores:
@@ -427,7 +588,10 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="decimal", choices=["decimal", "plain", "highcard"])
+    ap.add_argument("--workload", default="decimal", choices=["decimal", "plain", "highcard", "batched", "serving"])
+    ap.add_argument("--instances", type=int, default=512, help="batched: instances")
+    ap.add_argument("--rate", type=float, default=2000.0, help="serving: requests/s")
+    ap.add_argument("--seconds", type=float, default=10.0, help="serving: trace length")
     ap.add_argument("--rows", type=int, default=None)
     ap.add_argument("--chunk-rows", type=int, default=8 << 20)
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline sample length")
@@ -441,6 +605,11 @@ def main():
     if args.impl == "reference":
         if rank == 0:
             print(json.dumps(run_reference(args)), flush=True)
+        return
+    if args.workload in ("batched", "serving"):
+        if rank == 0:  # one GPU: these shapes are about one device's scheduling
+            fn = run_batched if args.workload == "batched" else run_serving
+            print(json.dumps(fn(args, local)), flush=True)
         return
 
     if world > 1:
