@@ -1274,12 +1274,15 @@ VR_DEV void private_to_global(const OpDesc& o, const uint64_t* hot, int nt, Cont
         case OP_COUNT_ROWS:
         case OP_COUNT_VALID:
         case OP_SUM_I32:
+            #pragma unroll 1  // once per CTA: keep it small
             for (int t = 0; t < nt; ++t) x.a += hot[t];
             break;
         case OP_MAX_KEY:
+            #pragma unroll 1  // once per CTA: keep it small
             for (int t = 0; t < nt; ++t) x.a = hot[t] > x.a ? hot[t] : x.a;
             break;
         case OP_MAX_D128:
+            #pragma unroll 1  // once per CTA: keep it small
             for (int t = 0; t < nt; ++t)
                 if (u128_gt(hot[t], hot[S + t], x.a, x.b)) {
                     x.a = hot[t];
@@ -1288,6 +1291,7 @@ VR_DEV void private_to_global(const OpDesc& o, const uint64_t* hot, int nt, Cont
             break;
         case OP_SUM_F64: {
             double s = 0.0, c = 0.0;
+            #pragma unroll 1  // once per CTA: keep it small
             for (int t = 0; t < nt; ++t) dd_add(s, c, as_f64(hot[t]), as_f64(hot[S + t]));
             x.a = as_u64(s);
             x.b = as_u64(c);
@@ -1297,6 +1301,7 @@ VR_DEV void private_to_global(const OpDesc& o, const uint64_t* hot, int nt, Cont
         case OP_SUM_PROD: {
             Acc192 a;
             acc_zero(a);
+            #pragma unroll 1  // once per CTA: keep it small
             for (int t = 0; t < nt; ++t) acc_add_i64(a, (int64_t)hot[t]);
             acc_to_cs(a, x.a, x.b);
             break;
@@ -1306,13 +1311,16 @@ VR_DEV void private_to_global(const OpDesc& o, const uint64_t* hot, int nt, Cont
         case OP_MERGE_DAVG: {
             Acc192 a;
             acc_zero(a);
+            #pragma unroll 1  // once per CTA: keep it small
             for (int t = 0; t < nt; ++t) acc_add_i128(a, hot[t], hot[S + t]);
             acc_to_limbs(a, x.a, x.b, x.c, x.d);
             if (K == OP_MERGE_DSUM) {
+                #pragma unroll 1  // once per CTA: keep it small
                 for (int t = 0; t < nt; ++t) x.e |= hot[2 * S + t];
             } else if (K == OP_MERGE_DAVG) {
                 Acc192 n;
                 acc_zero(n);
+                #pragma unroll 1  // once per CTA: keep it small
                 for (int t = 0; t < nt; ++t) acc_add_i64(n, (int64_t)hot[2 * S + t]);
                 acc_to_cs(n, x.e, x.f);
             }

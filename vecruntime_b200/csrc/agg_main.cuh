@@ -41,6 +41,7 @@ VR_DEV void set_error(uint64_t* ctrl, uint64_t bits) { atomicOr((unsigned long l
 VR_DEV void coop_copy(void* dst, const void* src, int bytes, int tid, int nt) {
     const uint64_t* s = reinterpret_cast<const uint64_t*>(src);
     uint64_t* d = reinterpret_cast<uint64_t*>(dst);
+    #pragma unroll 1  // once per CTA: keep it small
     for (int i = tid; i < bytes / 8; i += nt) d[i] = s[i];
 }
 
@@ -210,6 +211,25 @@ VR_DEV void jit_pack_key(const TileView& v, int64_t r, uint64_t (&k)[KW], bool& 
 #define VR_NUM_OPS(P) ((P).num_ops)
 #endif
 
+// Launch and layout constants: compile-time in a per-spec kernel (so the
+// compiler sees, e.g., that two ops' accumulator words never alias), read
+// from the Program / launch config in the prebuilt one.
+#ifdef VR_JIT
+#define VR_THREADS(cfg) VR_JIT_THREADS
+#define VR_PKW(P) VR_JIT_KW
+#define VR_PHW(P) VR_JIT_HW
+#define VR_PAW(P) VR_JIT_AW
+#define VR_PSW(P) VR_JIT_SW
+#define VR_PDSLOTS(P) ((int64_t)VR_JIT_DSLOTS)
+#else
+#define VR_THREADS(cfg) ((cfg).consumer_threads)
+#define VR_PKW(P) ((P).kw)
+#define VR_PHW(P) ((P).hw)
+#define VR_PAW(P) ((P).aw)
+#define VR_PSW(P) ((P).sw)
+#define VR_PDSLOTS(P) ((P).direct_slots)
+#endif
+
 // f(op, KindTag<op kind>{}) for op i: the per-spec constant descriptor under
 // VR_JIT, else the program's descriptor with its kind dispatched at run time.
 template <class F>
@@ -280,11 +300,11 @@ VR_DEV void hash_chunk(const Program& P, const BatchDesc& D, const TileView& v, 
         if (leader) {
             bool fresh = false, to = false;
             if (sslots > 0 && !side) {
-                slot[j] = find_or_insert<true, KW>(scache, sslots - 1, P.sw, key, h >> 32, false, s_probes, fresh, to);
+                slot[j] = find_or_insert<true, KW>(scache, sslots - 1, VR_PSW(P), key, h >> 32, false, s_probes, fresh, to);
                 in_smem[j] = slot[j] != nullptr;
             }
             if (!slot[j]) {
-                slot[j] = find_or_insert<false, KW>(D.table, D.cap_mask, P.sw, key, h, side, g_probes, fresh, to);
+                slot[j] = find_or_insert<false, KW>(D.table, D.cap_mask, VR_PSW(P), key, h, side, g_probes, fresh, to);
                 if (slot[j] && fresh) ++new_groups;
                 if (to) set_error(D.ctrl, kErrLockTimeout);
                 defer = (slot[j] == nullptr) && !to;
@@ -295,7 +315,7 @@ VR_DEV void hash_chunk(const Program& P, const BatchDesc& D, const TileView& v, 
             if (dm) defer = live[j] && ((dm >> (__ffs(peers) - 1)) & 1u);
         }
         if (defer) defer_row(D, row_base + r[j]);
-        if (slot[j]) slot[j] += P.kw;  // accumulator words
+        if (slot[j]) slot[j] += VR_PKW(P);  // accumulator words
     }
     VR_UNROLL
     for (int i = 0; i < VR_NUM_OPS(P); ++i)
@@ -323,7 +343,7 @@ VR_DEV void direct_chunk(const Program& P, const BatchDesc& D, const TileView& v
 #else
             int64_t gi = direct_index(P, v, r[j]);
 #endif
-            if (gi < 0 || gi >= P.direct_slots) {
+            if (gi < 0 || gi >= VR_PDSLOTS(P)) {
                 set_error(D.ctrl, kErrBadKey);
                 live[j] = false;
             } else {
@@ -331,7 +351,7 @@ VR_DEV void direct_chunk(const Program& P, const BatchDesc& D, const TileView& v
             }
         }
     }
-    const int hw = P.hw, aw = P.aw;
+    const int hw = VR_PHW(P), aw = VR_PAW(P);
     VR_UNROLL
     for (int i = 0; i < VR_NUM_OPS(P); ++i)
         for_op(P, i, [&](const OpDesc& op, auto tag) {
@@ -343,32 +363,33 @@ VR_DEV void direct_chunk(const Program& P, const BatchDesc& D, const TileView& v
 // combines the op's hot words over all consumer threads, adds the CTA's cold
 // words, and applies both to the dense HBM table with atomics.
 VR_DEV void flush_direct(const Program& P, const BatchDesc& D, uint64_t* priv, uint64_t* cold, int nt, int ctid) {
-    const int64_t G = P.direct_slots;
+    const int64_t G = VR_PDSLOTS(P);
     const int nops = P.num_ops;
+    #pragma unroll 1  // once per CTA: keep it small
     for (int64_t q = ctid; q < G * nops; q += nt) {
         int64_t g = q / nops;
-        uint64_t* gslot = D.table + (size_t)g * P.sw;
+        uint64_t* gslot = D.table + (size_t)g * VR_PSW(P);
         Contrib c;
         bool rows_op = false;
         for_op(P, (int)(q % nops), [&](const OpDesc& o, auto tag) {
             constexpr int K = decltype(tag)::value;
-            private_to_global<K>(o, priv + ((size_t)g * P.hw + o.hword) * nt, nt, c);
-            apply_global<K, false>(o, gslot + P.kw + o.word, c);
+            private_to_global<K>(o, priv + ((size_t)g * VR_PHW(P) + o.hword) * nt, nt, c);
+            apply_global<K, false>(o, gslot + VR_PKW(P) + o.word, c);
             Contrib cc;
-            load_state(o, cold + (size_t)g * P.aw + o.word, cc);
-            apply_global<K, false>(o, gslot + P.kw + o.word, cc);
+            load_state(o, cold + (size_t)g * VR_PAW(P) + o.word, cc);
+            apply_global<K, false>(o, gslot + VR_PKW(P) + o.word, cc);
             rows_op = K == OP_COUNT_ROWS;
         });
         if (rows_op && c.a != 0) {  // the group exists: store its key (same bits from every CTA)
             uint64_t kbuf[kMaxKW];
             direct_key(P, g, kbuf);
-            for (int i = 0; i < P.kw; ++i) gslot[i] = kbuf[i];
+            for (int i = 0; i < VR_PKW(P); ++i) gslot[i] = kbuf[i];
         }
     }
 }
 
 // Is slot occupied? Every live group has COUNT_ROWS (word 0) >= 1.
-VR_DEV bool slot_used(const Program& P, const uint64_t* slot) { return slot[P.kw] != 0; }
+VR_DEV bool slot_used(const Program& P, const uint64_t* slot) { return slot[VR_PKW(P)] != 0; }
 
 // Merges one slot state (key + accumulators) into the HBM table of D.
 // Returns false when the table had no room.
@@ -380,7 +401,7 @@ VR_DEV bool merge_state(const Program& P, const BatchDesc& D, const uint64_t* sr
     for (int i = 0; i < KW; ++i) key[i] = src[i];
     bool side = (P.occ_word < 0) && key[0] == 0;  // sentinel layout: stored 0 == the sentinel key
     bool fresh = false, to = false;
-    uint64_t* slot = find_or_insert<false, KW>(D.table, D.cap_mask, P.sw, key, hash_key<KW>(key), side, g_probes,
+    uint64_t* slot = find_or_insert<false, KW>(D.table, D.cap_mask, VR_PSW(P), key, hash_key<KW>(key), side, g_probes,
                                                fresh, to);
     if (to) set_error(D.ctrl, kErrLockTimeout);
     if (!slot) return false;
@@ -400,14 +421,15 @@ VR_DEV bool merge_state(const Program& P, const BatchDesc& D, const uint64_t* sr
 template <int KW>
 VR_DEV void flush_hash(const Program& P, const BatchDesc& D, uint64_t* scache, int sslots, int nt, int ctid,
                        uint32_t& new_groups, int g_probes) {
+    #pragma unroll 1  // once per CTA: keep it small
     for (int i = ctid; i < sslots; i += nt) {
-        const uint64_t* s = scache + (size_t)i * P.sw;
+        const uint64_t* s = scache + (size_t)i * VR_PSW(P);
         if (!slot_used(P, s)) continue;
         if (!merge_state<KW>(P, D, s, new_groups, g_probes)) {
             unsigned long long k = atomicAdd((unsigned long long*)&D.ctrl[CTRL_SPILLED], 1ull);
             if ((int64_t)k < D.spill_cap) {
-                uint64_t* dst = D.spill + (size_t)k * P.sw;
-                for (int w = 0; w < P.sw; ++w) dst[w] = s[w];
+                uint64_t* dst = D.spill + (size_t)k * VR_PSW(P);
+                for (int w = 0; w < VR_PSW(P); ++w) dst[w] = s[w];
             } else {
                 set_error(D.ctrl, kErrSpillFull);
             }
@@ -416,6 +438,7 @@ VR_DEV void flush_hash(const Program& P, const BatchDesc& D, uint64_t* scache, i
 }
 
 VR_DEV void zero_words(uint64_t* p, int64_t n, int tid, int nt) {
+    #pragma unroll 1  // once per CTA: keep it small
     for (int64_t i = tid; i < n; i += nt) p[i] = 0;
 }
 
@@ -442,7 +465,7 @@ VR_DEV void consume_tile(const Program& P, const BatchDesc& D, const LaunchCfg& 
                 r[j] = base + j * NT + ctid;
                 live[j] = r[j] < rows && (v.sel == nullptr || bit_at(v.sel, r[j]));
             }
-            direct_chunk<R>(P, D, v, r, live, tier, tier + (size_t)P.direct_slots * P.hw * NT, NT, ctid);
+            direct_chunk<R>(P, D, v, r, live, tier, tier + (size_t)VR_PDSLOTS(P) * VR_PHW(P) * NT, NT, ctid);
         }
     } else {
         const int ss = D.smem_slots < sslots ? D.smem_slots : sslots;
@@ -476,7 +499,7 @@ VR_DEV void aggregate_body(const BatchDesc* __restrict__ descs, const LaunchCfg&
     uint64_t* tier = reinterpret_cast<uint64_t*>(smem + m.tier);
 
     const int tid = threadIdx.x;
-    const int NT = cfg.consumer_threads;
+    const int NT = VR_THREADS(cfg);
 #ifndef VR_JIT
     coop_copy(smem + m.prog, descs[0].prog, (int)sizeof(Program), tid, blockDim.x);
 #endif
@@ -497,7 +520,7 @@ VR_DEV void aggregate_body(const BatchDesc* __restrict__ descs, const LaunchCfg&
 
     // consumer warps
     const int ctid = tid;
-    const int sslots = cfg.tier_bytes / (8 * P.sw);
+    const int sslots = cfg.tier_bytes / (8 * VR_PSW(P));
     int cur = -1;
     uint32_t new_groups = 0;
     for (int64_t k = 0;; ++k) {
@@ -515,7 +538,7 @@ VR_DEV void aggregate_body(const BatchDesc* __restrict__ descs, const LaunchCfg&
             consumer_bar(NT);
             if (cur >= 0) {
                 if (TIER == kTierDirect) {
-                    flush_direct(P, D, tier, tier + (size_t)P.direct_slots * P.hw * NT, NT, ctid);
+                    flush_direct(P, D, tier, tier + (size_t)VR_PDSLOTS(P) * VR_PHW(P) * NT, NT, ctid);
                 } else {
                     flush_hash<KW>(P, D, tier, D.smem_slots < sslots ? D.smem_slots : sslots, NT, ctid, new_groups,
                                    cfg.g_probes);
@@ -549,7 +572,7 @@ VR_DEV void aggregate_body(const BatchDesc* __restrict__ descs, const LaunchCfg&
     if (cur >= 0) {
         consumer_bar(NT);
         if (TIER == kTierDirect) {
-            flush_direct(P, D, tier, tier + (size_t)P.direct_slots * P.hw * NT, NT, ctid);
+            flush_direct(P, D, tier, tier + (size_t)VR_PDSLOTS(P) * VR_PHW(P) * NT, NT, ctid);
         } else {
             flush_hash<KW>(P, D, tier, D.smem_slots < sslots ? D.smem_slots : sslots, NT, ctid, new_groups,
                            cfg.g_probes);

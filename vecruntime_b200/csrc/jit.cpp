@@ -31,6 +31,7 @@ struct JitKernel {
     CUfunction fn = nullptr;
     int regs = 0;
     int smem_set = 0;
+    int threads = 0;  // consumer threads it was compiled for (a compile-time constant inside)
 };
 
 namespace {
@@ -268,6 +269,10 @@ static std::string jit_source(const Program& P, const JitShape& S) {
     std::string src = kPrelude;
     src += "#define VR_JIT_KW " + std::to_string(S.kw) + "\n#define VR_JIT_TIER " + std::to_string(S.tier) + "\n";
     src += "#define VR_JIT_RCHUNK " + std::to_string(S.rchunk) + "\n";
+    src += "#define VR_JIT_THREADS " + std::to_string(S.threads) + "\n";
+    src += "#define VR_JIT_HW " + std::to_string(P.hw) + "\n#define VR_JIT_AW " + std::to_string(P.aw) + "\n";
+    src += "#define VR_JIT_SW " + std::to_string(P.sw) + "\n#define VR_JIT_DSLOTS " +
+           std::to_string((long long)P.direct_slots) + "LL\n";
     src += "#define VR_JIT_NUM_OPS " + std::to_string(P.num_ops) + "\n";
     src += "#include \"agg_device.cuh\"\nnamespace vr {\n__constant__ const Program kJitProg = ";
     src += program_literal(P);
@@ -328,6 +333,7 @@ JitKernel* jit_get(const Program& P, const JitShape& S, int device, std::string*
     CUresult r = d.load(&k->mod, cubin.data());
     if (r == CUDA_SUCCESS) r = d.getfn(&k->fn, k->mod, "vr_jit_aggregate");
     if (r == CUDA_SUCCESS) r = d.getattr(&k->regs, CU_FUNC_ATTRIBUTE_NUM_REGS, k->fn);
+    k->threads = S.threads;
     cudaSetDevice(prev);
     if (r != CUDA_SUCCESS) {
         *err = "loading the compiled kernel failed (CUresult " + std::to_string((int)r) + ")";
@@ -343,6 +349,7 @@ int jit_regs(const JitKernel* k) { return k ? k->regs : 0; }
 cudaError_t jit_launch(JitKernel* k, const BatchDesc* descs, const LaunchCfg& cfg, int blocks, uint64_t* tile_counter,
                        cudaStream_t stream) {
     Driver& d = driver();
+    if (cfg.consumer_threads != k->threads) return cudaErrorInvalidConfiguration;  // compiled for another shape
     if (k->smem_set < cfg.smem_bytes) {
         if (d.setattr(k->fn, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, cfg.smem_bytes) != CUDA_SUCCESS)
             return cudaErrorInvalidValue;
