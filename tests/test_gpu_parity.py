@@ -6,6 +6,7 @@ import numpy as np
 import pytest
 
 import vecruntime_b200 as vr
+from vecruntime_b200 import aggregate as A
 from vecruntime_b200 import columns as Cc
 from vecruntime_b200 import datagen as G
 from vecruntime_b200 import native as N
@@ -142,3 +143,41 @@ def test_row_hash_matches_the_oracle(cuda, finish):
     torch.cuda.synchronize()
     got = out.cpu().numpy().view(np.uint32)
     assert np.array_equal(got, want), f"{int((got != want).sum())} of {n} hashes differ"
+
+
+def dictionary_workload(rows, seed, with_nulls=True):
+    """Two dictionary keys (5 and 3 ids, nullable), an int64 value with nulls,
+    a double, decimal columns for a fused product: the direct tier's shape
+    with everything that can make a row not count."""
+    rng = np.random.default_rng(seed)
+    n1 = rng.random(rows) < (0.1 if with_nulls else 0)
+    n2 = rng.random(rows) < (0.05 if with_nulls else 0)
+    cols = [Cc.dict_ids(rng.integers(0, 5, rows), 5, n1, nullable=True),
+            Cc.dict_ids(rng.integers(0, 3, rows), 3, n2, nullable=True),
+            Cc.longs(rng.integers(-(1 << 40), 1 << 40, rows, dtype=np.int64), rng.random(rows) < 0.1, nullable=True),
+            Cc.doubles(rng.standard_normal(rows), nullable=False),
+            Cc.decimals(rng.integers(0, 10**9, rows, dtype=np.int64), 12, 2, nullable=False),
+            Cc.decimals(rng.integers(0, 11, rows, dtype=np.int64), 12, 2, nullable=False)]
+    fns = [A.CountAgg(), A.CountAgg(2), A.SumLongAgg(2), A.SumDoubleAgg(3), A.MinMaxAgg(2, True),
+           A.MinMaxAgg(2, False), A.WideDecimalSumAgg(A.DecimalProduct([(4, 1, 0), (5, -1, 100)], precision=26), 36, 4)]
+    return G.Workload("dict", cols, [0, 1], fns, 24, rows)
+
+
+@pytest.mark.parametrize("rows", [1, 777, 100_003])
+def test_direct_tier_with_selection_nulls_and_partial_tiles(cuda, rows):
+    w = dictionary_workload(rows, 900 + rows)
+    sel = Cc.pack_bits(np.random.default_rng(rows).random(rows) < 0.6)
+    batches = [w.batch(0, rows, selection=sel)]
+    st = check(w, batches)
+    assert st.tier == 0, "expected the direct tier"
+
+
+def test_direct_tier_id_outside_its_dictionary_is_an_error(cuda):
+    w = dictionary_workload(5000, 5)
+    w.columns[1].data[4321] = 7  # dictionary size 3
+    agg = vr.GpuHashAggregate(w.columns, w.keys, w.functions, est_groups=w.est_groups, max_batch_rows=w.rows)
+    with pytest.raises(vr.VrError) as e:
+        agg.consume(w.batch())
+        agg.sync()
+    assert e.value.status == N.VR_ERR_INVALID
+    agg.close()

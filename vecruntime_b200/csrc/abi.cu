@@ -139,8 +139,9 @@ static int choose_config(vr_agg* h, const vr_tune_choice* forced) {
         const int Rs[] = {8, 4, 2};
         for (int nt : nts) {
             if (forced && forced->threads && nt != forced->threads) continue;
-            // thread-private hot words + the CTA's cold words
-            int64_t tb = (P.direct_slots * P.hw * (int64_t)nt + P.direct_slots * P.aw) * 8;
+            // thread-private hot words + the CTA's cold words, for every
+            // group and the trash group that rows which do not count go to
+            int64_t tb = ((P.direct_slots + 1) * P.hw * (int64_t)nt + (P.direct_slots + 1) * P.aw) * 8;
             if (tb > budget) continue;
             for (int R : Rs) {
                 const int T = nt * R;
@@ -233,7 +234,7 @@ static int choose_config(vr_agg* h, const vr_tune_choice* forced) {
     if (forced) c.warp_agg = forced->warp_agg;
     if (fl & VR_SPEC_NO_TMA) c.tma = 0;
     const int tier_bytes = c.tier == kTierDirect
-                               ? (int)((P.direct_slots * P.hw * (int64_t)c.threads + P.direct_slots * P.aw) * 8)
+                               ? (int)(((P.direct_slots + 1) * P.hw * (int64_t)c.threads + (P.direct_slots + 1) * P.aw) * 8)
                                : c.smem_slots * P.sw * 8;
     SmemMap m = smem_map(c.stages, stage_bytes_for(P, c.tile_rows), tier_bytes);
     // blocks per SM: shared memory and registers (the ahead-of-time kernel's;

@@ -179,21 +179,91 @@ VR_DEV void hash_op(const OpDesc& op, const TileView& v, const int64_t (&r)[R], 
     }
 }
 
+// Kinds whose thread-private update is one int64 add per row.
+template <int K>
+struct OneAdd {
+    static constexpr bool value =
+        K == OP_COUNT_ROWS || K == OP_COUNT_VALID || K == OP_SUM_I32 || K == OP_SUM_I64 || K == OP_SUM_PROD;
+};
+
+// A OneAdd kind's value for row r without branches. `exact` false sends the
+// row to the exact path instead (a null product factor, a product past int64
+// or past its precision); the value is then 0.
+template <int K, class V>
+VR_DEV int64_t fast_value(const OpDesc& o, const V& v, int64_t r, bool& exact) {
+    exact = true;
+    switch (K) {
+        case OP_COUNT_ROWS:
+            return 1;
+        case OP_COUNT_VALID:
+            return (o.nterms > 0 ? terms_valid(o, v, r) : in_valid(o, v, o.col, r)) ? 1 : 0;
+        case OP_SUM_I32:
+            return in_valid(o, v, o.col, r) ? (int64_t)ld_i32(v, o.col, r) : 0;
+        case OP_SUM_I64:
+            return in_valid(o, v, o.col, r) ? ld_int(v, o.col, o.lane, r) : 0;
+        case OP_SUM_PROD: {
+            const int64_t a = term_value(o, v, r, 0), b = term_value(o, v, r, 1);
+            int64_t p = a * b;
+            bool fits = __mul64hi(a, b) == (p >> 63);
+            if (o.nterms == 3) {
+                const int64_t c = term_value(o, v, r, 2);
+                const int64_t q = p * c;
+                fits = fits && __mul64hi(p, c) == (q >> 63);
+                p = q;
+            }
+            exact = fits && within_precision64(p, o.prec) && terms_valid(o, v, r);
+            return exact ? p : 0;
+        }
+    }
+    return 0;
+}
+
 // One op over a direct-tier chunk: thread-private hot words, CTA cold words.
+// Rows that must not count (past the tile, unselected, a key outside its
+// dictionary) arrive with the trash group, so the fast path has no branch per
+// row: one int64 add into the row's hot word, its signed wrap and any need
+// for the exact path noted in bit masks, handled after the chunk (rare).
 template <int K, int R>
-VR_DEV void direct_op(const OpDesc& op, const TileView& v, const int64_t (&r)[R], const bool (&live)[R],
-                      const int (&g)[R], uint64_t* priv, uint64_t* cold, int nt, int ctid, int hw, int aw) {
+VR_DEV void direct_op(const OpDesc& op, const TileView& v, const int64_t (&r)[R], const int (&g)[R], uint64_t* priv,
+                      uint64_t* cold, int nt, int ctid, int hw, int aw) {
     OpDesc o;
     OpView ov;
     make_opview(op, v, o, ov);
     uint64_t* hot = priv + (size_t)o.hword * nt + ctid;
     uint64_t* cop = cold + o.word;
     const size_t gstride = (size_t)hw * nt;
+    if constexpr (OneAdd<K>::value) {
+        constexpr bool kWraps = K == OP_SUM_I64 || K == OP_SUM_PROD;
+        uint32_t rare = 0, wrap = 0;
+        int64_t x[R];
 #pragma unroll
-    for (int j = 0; j < R; ++j) {
-        Contrib c;
-        if (live[j] && op_raw<K>(o, ov, r[j], c))
-            apply_private<K>(o, hot + g[j] * gstride, nt, cop + (size_t)g[j] * aw, c);
+        for (int j = 0; j < R; ++j) {
+            bool exact;
+            x[j] = fast_value<K>(o, ov, r[j], exact);
+            uint64_t* h = hot + g[j] * gstride;
+            const int64_t s = (int64_t)*h;
+            const int64_t ns = (int64_t)((uint64_t)s + (uint64_t)x[j]);
+            *h = (uint64_t)ns;
+            if (kWraps) wrap |= (uint32_t)(((s ^ ns) & (x[j] ^ ns)) < 0) << j;
+            rare |= (uint32_t)!exact << j;
+        }
+        if (rare | wrap) {
+#pragma unroll
+            for (int j = 0; j < R; ++j) {
+                if ((wrap >> j) & 1u)  // +-2^64 into the carry-save high word (+-2^32 there)
+                    s_add(cop + (size_t)g[j] * aw + 1, x[j] > 0 ? (1ull << 32) : (0ull - (1ull << 32)));
+                if ((rare >> j) & 1u) {
+                    Contrib c;
+                    if (op_raw<K>(o, ov, r[j], c)) apply_private<K>(o, hot + g[j] * gstride, nt, cop + (size_t)g[j] * aw, c);
+                }
+            }
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+            Contrib c;
+            if (op_raw<K>(o, ov, r[j], c)) apply_private<K>(o, hot + g[j] * gstride, nt, cop + (size_t)g[j] * aw, c);
+        }
     }
 }
 
@@ -330,32 +400,27 @@ VR_DEV void hash_chunk(const Program& P, const BatchDesc& D, const TileView& v, 
 // (kind fixed at compile time, column pointers in registers).
 template <int R>
 VR_DEV void direct_chunk(const Program& P, const BatchDesc& D, const TileView& v, const int64_t (&r)[R],
-                         const bool (&live_in)[R], uint64_t* priv, uint64_t* cold, int nt, int ctid) {
-    bool live[R];
+                         const bool (&live)[R], uint64_t* priv, uint64_t* cold, int nt, int ctid) {
     int g[R];
+    uint32_t bad = 0;
 #pragma unroll
     for (int j = 0; j < R; ++j) {
-        live[j] = live_in[j];
-        g[j] = 0;
-        if (live[j]) {
 #ifdef VR_JIT
-            int64_t gi = jit_direct_index(v, r[j]);
+        const int64_t gi = jit_direct_index(v, r[j]);
 #else
-            int64_t gi = direct_index(P, v, r[j]);
+        const int64_t gi = direct_index(P, v, r[j]);
 #endif
-            if (gi < 0 || gi >= VR_PDSLOTS(P)) {
-                set_error(D.ctrl, kErrBadKey);
-                live[j] = false;
-            } else {
-                g[j] = (int)gi;
-            }
-        }
+        const bool ok = gi >= 0 && gi < VR_PDSLOTS(P);
+        bad |= (uint32_t)(live[j] && !ok) << j;
+        // rows that do not count accumulate into the trash group (never flushed)
+        g[j] = live[j] && ok ? (int)gi : (int)VR_PDSLOTS(P);
     }
+    if (bad) set_error(D.ctrl, kErrBadKey);
     const int hw = VR_PHW(P), aw = VR_PAW(P);
     VR_UNROLL
     for (int i = 0; i < VR_NUM_OPS(P); ++i)
         for_op(P, i, [&](const OpDesc& op, auto tag) {
-            direct_op<decltype(tag)::value, R>(op, v, r, live, g, priv, cold, nt, ctid, hw, aw);
+            direct_op<decltype(tag)::value, R>(op, v, r, g, priv, cold, nt, ctid, hw, aw);
         });
 }
 
@@ -462,10 +527,11 @@ VR_DEV void consume_tile(const Program& P, const BatchDesc& D, const LaunchCfg& 
             bool live[R];
 #pragma unroll
             for (int j = 0; j < R; ++j) {
-                r[j] = base + j * NT + ctid;
-                live[j] = r[j] < rows && (v.sel == nullptr || bit_at(v.sel, r[j]));
+                const int64_t rr = base + j * NT + ctid;
+                live[j] = rr < rows && (v.sel == nullptr || bit_at(v.sel, rr));
+                r[j] = rr < rows ? rr : rows - 1;  // past the tile: a real row, counted into the trash group
             }
-            direct_chunk<R>(P, D, v, r, live, tier, tier + (size_t)VR_PDSLOTS(P) * VR_PHW(P) * NT, NT, ctid);
+            direct_chunk<R>(P, D, v, r, live, tier, tier + (size_t)(VR_PDSLOTS(P) + 1) * VR_PHW(P) * NT, NT, ctid);
         }
     } else {
         const int ss = D.smem_slots < sslots ? D.smem_slots : sslots;
@@ -538,7 +604,7 @@ VR_DEV void aggregate_body(const BatchDesc* __restrict__ descs, const LaunchCfg&
             consumer_bar(NT);
             if (cur >= 0) {
                 if (TIER == kTierDirect) {
-                    flush_direct(P, D, tier, tier + (size_t)VR_PDSLOTS(P) * VR_PHW(P) * NT, NT, ctid);
+                    flush_direct(P, D, tier, tier + (size_t)(VR_PDSLOTS(P) + 1) * VR_PHW(P) * NT, NT, ctid);
                 } else {
                     flush_hash<KW>(P, D, tier, D.smem_slots < sslots ? D.smem_slots : sslots, NT, ctid, new_groups,
                                    cfg.g_probes);
@@ -572,7 +638,7 @@ VR_DEV void aggregate_body(const BatchDesc* __restrict__ descs, const LaunchCfg&
     if (cur >= 0) {
         consumer_bar(NT);
         if (TIER == kTierDirect) {
-            flush_direct(P, D, tier, tier + (size_t)VR_PDSLOTS(P) * VR_PHW(P) * NT, NT, ctid);
+            flush_direct(P, D, tier, tier + (size_t)(VR_PDSLOTS(P) + 1) * VR_PHW(P) * NT, NT, ctid);
         } else {
             flush_hash<KW>(P, D, tier, D.smem_slots < sslots ? D.smem_slots : sslots, NT, ctid, new_groups,
                            cfg.g_probes);
