@@ -200,6 +200,7 @@ static int choose_config(vr_agg* h, const vr_tune_choice* forced) {
                             c.tile_rows = T;
                             c.stages = st;
                             c.smem_slots = (int)need;
+                            c.s_probes = 64;  // at most half full: every key finds its place
                             done = true;
                         }
                     }
@@ -222,6 +223,9 @@ static int choose_config(vr_agg* h, const vr_tune_choice* forced) {
             if (use_cache && slots >= 64) {
                 int64_t want = forced && forced->smem_slots ? next_pow2(forced->smem_slots) : std::min<int64_t>(need, 256);
                 c.smem_slots = (int)std::min(slots, want);
+                // keys settle within two slots of home or not at all, so a miss
+                // (most rows once the cache is full) costs two probes
+                c.s_probes = 2;
             }
         }
         // warp pre-aggregation pays only when rows of a warp often share a

@@ -122,6 +122,34 @@ VR_DEV uint64_t s_cas(uint64_t* p, uint64_t cmp, uint64_t val) {
 VR_DEV void g_add(uint64_t* p, uint64_t v) { atomicAdd((unsigned long long*)p, (unsigned long long)v); }
 VR_DEV void g_max(uint64_t* p, uint64_t v) { atomicMax((unsigned long long*)p, (unsigned long long)v); }
 VR_DEV void g_or(uint64_t* p, uint64_t v) { atomicOr((unsigned long long*)p, (unsigned long long)v); }
+
+// Reductions skipped for a zero operand by a predicate on the instruction
+// itself, not a branch around it (rows contribute zero words often: the high
+// half of a small sum, a count of a valid value).
+VR_DEV void s_add_nz(uint64_t* p, uint64_t v) {
+    asm volatile("{ .reg .pred q; setp.ne.u64 q, %1, 0; @q red.shared.add.u64 [%0], %1; }" ::"r"(smem_u32(p)), "l"(v)
+                 : "memory");
+}
+VR_DEV void s_max_nz(uint64_t* p, uint64_t v) {
+    asm volatile("{ .reg .pred q; setp.ne.u64 q, %1, 0; @q red.shared.max.u64 [%0], %1; }" ::"r"(smem_u32(p)), "l"(v)
+                 : "memory");
+}
+VR_DEV void s_or_nz(uint64_t* p, uint64_t v) {
+    asm volatile("{ .reg .pred q; setp.ne.u64 q, %1, 0; @q red.shared.or.b64 [%0], %1; }" ::"r"(smem_u32(p)), "l"(v)
+                 : "memory");
+}
+VR_DEV void g_add_nz(uint64_t* p, uint64_t v) {
+    asm volatile("{ .reg .pred q; setp.ne.u64 q, %1, 0; @q red.relaxed.gpu.global.add.u64 [%0], %1; }" ::"l"(p), "l"(v)
+                 : "memory");
+}
+VR_DEV void g_max_nz(uint64_t* p, uint64_t v) {
+    asm volatile("{ .reg .pred q; setp.ne.u64 q, %1, 0; @q red.relaxed.gpu.global.max.u64 [%0], %1; }" ::"l"(p), "l"(v)
+                 : "memory");
+}
+VR_DEV void g_or_nz(uint64_t* p, uint64_t v) {
+    asm volatile("{ .reg .pred q; setp.ne.u64 q, %1, 0; @q red.relaxed.gpu.global.or.b64 [%0], %1; }" ::"l"(p), "l"(v)
+                 : "memory");
+}
 VR_DEV double g_fadd(double* p, double v) { return atomicAdd(p, v); }
 VR_DEV uint64_t g_cas(uint64_t* p, uint64_t cmp, uint64_t val) {
     return (uint64_t)atomicCAS((unsigned long long*)p, (unsigned long long)cmp, (unsigned long long)val);
@@ -184,6 +212,9 @@ VR_DEV uint64_t ld_relaxed_g(const uint64_t* p) {
 // Address-space dispatch: S = true for shared memory, false for global.
 template <bool S> struct Mem;
 template <> struct Mem<true> {
+    static VR_DEV void add_nz(uint64_t* p, uint64_t v) { s_add_nz(p, v); }
+    static VR_DEV void max_nz(uint64_t* p, uint64_t v) { s_max_nz(p, v); }
+    static VR_DEV void bor_nz(uint64_t* p, uint64_t v) { s_or_nz(p, v); }
     static VR_DEV void add(uint64_t* p, uint64_t v) { s_add(p, v); }
     static VR_DEV void max(uint64_t* p, uint64_t v) { s_max(p, v); }
     static VR_DEV void bor(uint64_t* p, uint64_t v) { s_or(p, v); }
@@ -197,6 +228,9 @@ template <> struct Mem<true> {
     }
 };
 template <> struct Mem<false> {
+    static VR_DEV void add_nz(uint64_t* p, uint64_t v) { g_add_nz(p, v); }
+    static VR_DEV void max_nz(uint64_t* p, uint64_t v) { g_max_nz(p, v); }
+    static VR_DEV void bor_nz(uint64_t* p, uint64_t v) { g_or_nz(p, v); }
     static VR_DEV void add(uint64_t* p, uint64_t v) { g_add(p, v); }
     static VR_DEV void max(uint64_t* p, uint64_t v) { g_max(p, v); }
     static VR_DEV void bor(uint64_t* p, uint64_t v) { g_or(p, v); }
@@ -1021,15 +1055,15 @@ VR_DEV void peer_reduce(const OpDesc& o, const PeerPlan& pp, Contrib& x) {
 // ----------------------------------------------------- atomic apply ----
 template <bool S>
 VR_DEV void add_nz(uint64_t* p, uint64_t v) {
-    if (v) Mem<S>::add(p, v);
+    Mem<S>::add_nz(p, v);
 }
 template <bool S>
 VR_DEV void or_nz(uint64_t* p, uint64_t v) {
-    if (v) Mem<S>::bor(p, v);
+    Mem<S>::bor_nz(p, v);
 }
 template <bool S>
 VR_DEV void max_nz(uint64_t* p, uint64_t v) {
-    if (v) Mem<S>::max(p, v);
+    Mem<S>::max_nz(p, v);
 }
 // Compensated atomic add of a double-double (s, c): the hardware add rounds to
 // nearest like __dadd_rn, so the thread recovers the exact rounding error of
