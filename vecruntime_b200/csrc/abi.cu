@@ -9,6 +9,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -255,6 +256,12 @@ static int choose_config(vr_agg* h, const vr_tune_choice* forced) {
     std::memset(&L, 0, sizeof(L));
     L.tile_rows = c.tile_rows;
     L.rchunk = c.rchunk;
+    // ~2 s at most per barrier wait (a stage normally arrives in microseconds);
+    // the test hooks shorten it and stop the producer, so a test can watch a
+    // wait run out and the error come back with the context still usable
+    L.wait_polls = 2048;
+    if (const char* e = std::getenv("VRGPU_TEST_WAIT_POLLS")) L.wait_polls = std::max(1, std::atoi(e));
+    if (const char* e = std::getenv("VRGPU_TEST_STALL_PRODUCER")) L.test_stall = std::atoi(e) != 0;
     L.stages = c.stages;
     L.consumer_threads = c.threads;
     L.num_desc = 1;

@@ -39,8 +39,7 @@ namespace vr {
 constexpr uint32_t kFull = 0xffffffffu;
 // Spin limits: every wait in these kernels gives up after this many polls and
 // reports kErrTimeout / kErrLockTimeout instead of hanging the device.
-constexpr uint32_t kWaitPolls = 1u << 14;
-constexpr uint32_t kSuspendHintNs = 1000000;  // 1 ms per poll
+constexpr uint32_t kSuspendHintNs = 1000000;  // at most 1 ms per poll
 constexpr uint32_t kLockPolls = 1u << 22;
 // Single 64-bit keys are stored xor this constant so that 0 means "empty";
 // the one key equal to it lives in an extra slot past the table's end.
@@ -79,10 +78,10 @@ VR_DEV bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-// Bounded wait: false when the poll budget ran out (kWaitPolls suspended
-// polls of up to kSuspendHintNs each: seconds, never forever).
-VR_DEV bool mbar_wait(uint64_t* bar, uint32_t parity) {
-    for (uint32_t i = 0; i < kWaitPolls; ++i)
+// Bounded wait: false when the poll budget ran out (`polls` suspended polls
+// of up to kSuspendHintNs each: about a second by default, never forever).
+VR_DEV bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t polls) {
+    for (uint32_t i = 0; i < polls; ++i)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }

@@ -69,12 +69,13 @@ VR_DEV void producer_loop(const Program& P, const BatchDesc* __restrict__ descs,
                           unsigned char* stage0, BatchDesc* pd) {
     const int NS = cfg.stages;
     const int T = cfg.tile_rows;
+    if (cfg.test_stall) return;  // test hook: nothing issued, nothing in flight
     int cur = -1;
     int64_t t_next = (int64_t)atomicAdd((unsigned long long*)tile_counter, 1ull);
     for (int64_t k = 0;; ++k) {
         int s = (int)(k % NS);
         uint32_t parity = (uint32_t)((k / NS) & 1);
-        if (!mbar_wait(&empty[s], parity ^ 1u)) {
+        if (!mbar_wait(&empty[s], parity ^ 1u, (uint32_t)cfg.wait_polls)) {
             set_error(descs[0].ctrl, kErrTimeout);
             return;
         }
@@ -592,7 +593,7 @@ VR_DEV void aggregate_body(const BatchDesc* __restrict__ descs, const LaunchCfg&
     for (int64_t k = 0;; ++k) {
         int s = (int)(k % cfg.stages);
         uint32_t parity = (uint32_t)((k / cfg.stages) & 1);
-        if (!mbar_wait(&full[s], parity)) {
+        if (!mbar_wait(&full[s], parity, (uint32_t)cfg.wait_polls)) {
             set_error(descs[0].ctrl, kErrTimeout);
             break;
         }
