@@ -18,7 +18,7 @@
 // 2296-2371) and the scatter loops of GroupedAccumulators
 // (GroupedAccumulators.java:252-300, 424-472, 563-601, 852-862, 1052-1069).
 #include <cub/device/device_select.cuh>
-#include <cub/iterator/counting_input_iterator.cuh>
+#include <thrust/iterator/counting_iterator.h>
 
 #include "agg_device.cuh"
 #include "agg_kernels.cuh"
@@ -487,7 +487,7 @@ cudaError_t launch_compact_kw(int kw, const uint64_t* table, int64_t slots, int 
     pred.table = table;
     pred.sw = sw;
     pred.kw = kw;
-    cub::CountingInputIterator<int64_t> it(0);
+    thrust::counting_iterator<int64_t> it(0);
     return cub::DeviceSelect::If(temp, *temp_bytes, it, out, num_dev, slots, pred, stream);
 }
 
