@@ -1062,6 +1062,13 @@ VR_DEV void or_nz(uint64_t* p, uint64_t v) {
 }
 template <bool S>
 VR_DEV void max_nz(uint64_t* p, uint64_t v) {
+    if (S) {
+        // A max only grows, so a value not above a (possibly stale) read of
+        // it cannot change it: after the first rows nearly every row skips
+        // its shared-memory atomic. HBM words keep the plain reduction (a
+        // read there is a round trip).
+        if (v <= *(const volatile uint64_t*)p) return;
+    }
     Mem<S>::max_nz(p, v);
 }
 // Compensated atomic add of a double-double (s, c): the hardware add rounds to
