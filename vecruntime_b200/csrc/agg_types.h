@@ -37,6 +37,7 @@ struct SmemMap {
 };
 
 constexpr int kMaxStages = 4;
-constexpr int kMaxConsumerThreads = 256;
+constexpr int kMaxConsumerThreads = 256;     // the prebuilt kernel's launch bounds
+constexpr int kMaxConsumerThreadsJit = 512;  // per-spec kernels take their bounds from the shape
 
 }  // namespace vr

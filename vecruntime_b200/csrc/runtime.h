@@ -116,6 +116,7 @@ struct vr_agg {
     bool trace = false;
     bool dead = false;
     vr::JitKernel* jit = nullptr;  // the spec's own kernel (owned by the process-wide cache)
+    bool prebuilt_only = false;    // no per-spec kernel: blocks stay within the prebuilt kernel's bounds
     std::string jit_error;         // why it could not be compiled, when it could not
 };
 
