@@ -244,7 +244,9 @@ int vr_agg_output_schema(const vr_agg* h, int32_t* num_out, vr_column_type* type
 int vr_agg_emit(vr_agg* h, int64_t from, int64_t to, const vr_out_column* outs, int32_t location);
 
 /* Empties the table, keeping its memory (EmitAndReset,
- *   VectorHashAggregateExec.scala:193-246). */
+ *   VectorHashAggregateExec.scala:193-246). A batch still in flight is
+ *   settled first; the clear itself is queued on the handle's stream, ahead
+ *   of later updates and emits, and does not wait for the device. */
 int vr_agg_reset(vr_agg* h);
 
 /* Frees device state (GroupedAggState.close, VectorAggregates.scala:85-90). */

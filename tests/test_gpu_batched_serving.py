@@ -39,6 +39,44 @@ def shared_choice():
     return t
 
 
+def test_reset_is_ordered_before_later_work(cuda):
+    """vr_agg_reset only queues its clear on the handle's stream: updates and
+    emits issued right after it, and a batched launch on another stream, must
+    all see an empty table."""
+    ws = G.batched_instances(n=6, max_log_rows=14, max_log_card=12)
+    aggs, dbs, keep = [], [], []
+    for w in ws:
+        aggs.append(vr.GpuHashAggregate(w.columns, w.keys, w.functions, est_groups=w.est_groups,
+                                        max_batch_rows=w.rows, tune=shared_choice()))
+        db, t = Cc.to_device(w.batch())
+        dbs.append(db)
+        keep.append(t)
+    try:
+        for a, db in zip(aggs, dbs):
+            a.consume(db)
+            a.consume(db)
+        for w, a, db in zip(ws, aggs, dbs):  # no sync between the clear and the next update
+            a.reset()
+            a.consume(db)
+            n = a.num_groups()
+            compare(w.spec(), a.output_types, a.emit(), n, *oracle_of(w, [w.batch()]))
+        for a, db in zip(aggs, dbs):
+            a.consume(db)
+        for a in aggs:
+            a.reset()
+        b = vr.GpuBatchedAggregate(aggs, dbs, mode=N.VR_BATCHED_PERSISTENT)
+        try:
+            b.run()
+            for w, a in zip(ws, aggs):
+                n = a.num_groups()
+                compare(w.spec(), a.output_types, a.emit(), n, *oracle_of(w, [w.batch()]))
+        finally:
+            b.close()
+    finally:
+        for a in aggs:
+            a.close()
+
+
 @pytest.mark.parametrize("mode,use_graph", [(N.VR_BATCHED_PERSISTENT, False), (N.VR_BATCHED_PERSISTENT, True),
                                             (N.VR_BATCHED_PLAIN, False)])
 def test_batched_instances_match_the_oracle(cuda, mode, use_graph):

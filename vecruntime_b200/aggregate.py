@@ -265,8 +265,9 @@ class GpuBatchedAggregate:
         self.h = h
 
     def run(self, stream: int = 0) -> None:
-        """Resets every instance's table and aggregates every instance's batch,
-        asynchronously on `stream` (0: the first instance's stream)."""
+        """Resets every instance's table and aggregates every instance's batch
+        on `stream` (0: the legacy default stream); returns once the device
+        has finished and every instance's group count is known."""
         rc = self._lib.vr_batched_run(self.h, C.c_void_p(stream) if stream else None)
         if rc:
             raise N.VrError(rc, "vr_batched_run: " + (self._lib.vr_thread_last_error() or b"").decode())

@@ -643,6 +643,7 @@ static int map_ctrl_error(vr_agg* h, uint64_t bits) {
 int agg_resolve_all(vr_agg* h) {
     cudaError_t e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return cuda_err(h, e, "update");
+    h->clear_queued = false;
     const Program& P = h->plan.prog;
     int order[2] = {h->next_slot, h->next_slot ^ 1};  // oldest first
     for (int k = 0; k < 2; ++k) {
@@ -979,11 +980,17 @@ int vr_agg_reset(vr_agg* h) {
     if (!h) return VR_ERR_INVALID;
     if (h->dead) return VR_ERR_STATE;
     cudaSetDevice(h->device);
-    int rc = agg_resolve_all(h);
-    if (rc != VR_OK) return rc;
+    // a pending batch may still grow the table or fail: settle it first;
+    // otherwise the clear is only queued behind earlier work on the stream
+    // (later updates and emits are ordered after it), so the device never
+    // idles while the host prepares the next launch
+    if (h->slot[0].pending || h->slot[1].pending) {
+        int rc = agg_resolve_all(h);
+        if (rc != VR_OK) return rc;
+    }
     cudaError_t e = cudaMemsetAsync(h->table, 0, (size_t)h->table_slots * h->plan.prog.sw * 8, h->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return cuda_err(h, e, "reset");
+    h->clear_queued = true;
     h->groups_known = 0;
     h->compact_valid = false;
     h->num_groups = 0;

@@ -212,6 +212,13 @@ int vr_batched_run(vr_batched* b, void* stream) {
     cudaStream_t st = (cudaStream_t)stream;
     cudaError_t e;
     int rc;
+    // the launch zeros every table on `st`: a clear still queued on an
+    // instance's own stream must not land in the middle of it
+    for (vr_agg* h : b->inst) {
+        if (!h->clear_queued) continue;
+        if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) return VR_ERR_CUDA;
+        h->clear_queued = false;
+    }
     if (b->use_graph) {
         if (!b->exec || b->graph_stream != st) {
             if (b->exec) cudaGraphExecDestroy(b->exec);

@@ -91,6 +91,7 @@ struct vr_agg {
     vr::StageSlot slot[2];
     int next_slot = 0;
     int64_t groups_known = 0;
+    bool clear_queued = false;  // vr_agg_reset's memset may still be in flight on `stream`
     // compaction / emission
     bool compact_valid = false;
     int64_t* slot_of = nullptr;
