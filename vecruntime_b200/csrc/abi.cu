@@ -111,6 +111,26 @@ cudaError_t agg_launch(vr_agg* h, const BatchDesc* descs, const LaunchCfg& L, in
     return launch_aggregate(h->plan.prog.kw, h->cfg.tier, descs, L, blocks, tile_counter, st);
 }
 
+// CTAs per SM by default, and the most a choice may ask for.
+constexpr int kDefaultCtasPerSm = 2;
+constexpr int kMaxCtasPerSm = 4;
+
+// How many CTAs of `threads` consumer threads (plus the producer warp), each
+// with `smem` dynamic shared bytes and `regs` registers per thread (0 =
+// unknown), fit on one SM together, at most `want`.
+static int ctas_per_sm(const DeviceInfo& di, int smem, int regs, int threads, int want) {
+    const int block = threads + 32;
+    const int rb = (regs + 7) / 8 * 8;
+    int k = 1;
+    while (k < want && di.fits(k + 1, smem) && (k + 1) * block <= 2048 && (regs <= 0 || (k + 1) * rb * block <= 65536))
+        ++k;
+    return k;
+}
+
+static int wanted_ctas(const vr_tune_choice* forced) {
+    return forced && forced->blocks_per_sm ? std::min<int>(forced->blocks_per_sm, kMaxCtasPerSm) : kDefaultCtasPerSm;
+}
+
 // Picks tier, block shape, tile and shared-cache sizes. `forced` (tests /
 // tuner) overrides the defaults field by field.
 static int choose_config(vr_agg* h, const vr_tune_choice* forced) {
@@ -137,13 +157,17 @@ static int choose_config(vr_agg* h, const vr_tune_choice* forced) {
         // thread), so no lane idles inside a full tile. Among the shapes that
         // fit, the most consumer threads per SM times rows in flight per
         // thread (up to 4) wins, two CTAs per SM on a tie. Measured on the
-        // decimal report (20M rows): 2 CTAs x 128 threads x 4 rows 0.32 ms,
-        // 1 x 256 x 4 0.35 ms, 1 x 128 x 8 0.50 ms, 1 x 256 x 2 0.51 ms.
-        const int nts[] = {256, 192, 128, 96, 64};
+        // decimal report (20M rows): 2 CTAs x 160 threads x 4 rows 0.297 ms,
+        // 3 x 96 x 4 0.301 ms, 4 x 64 x 4 0.310 ms, 2 x 128 x 4 0.321 ms,
+        // 1 x 256 x 4 0.35 ms, 1 x 224 x 4 0.37 ms, 2 x 96 x 4 0.38 ms,
+        // 1 x 128 x 8 0.50 ms, 1 x 256 x 2 0.51 ms. More than two CTAs per SM
+        // only on request (a tuning choice).
+        const int nts[] = {256, 224, 192, 160, 128, 96, 64};
         const int Rs[] = {4, 8, 2};
         int64_t best = -1;
-        for (int ctas = 2; ctas >= 1; --ctas) {
-            const int bytes = ctas == 2 ? std::min(budget, di.smem_per_sm / 2 - di.smem_reserved) : budget;
+        const int top = wanted_ctas(forced);
+        for (int ctas = top; ctas >= (forced && forced->blocks_per_sm ? top : 1); --ctas) {
+            const int bytes = ctas == 1 ? budget : std::min(budget, di.smem_per_sm / ctas - di.smem_reserved);
             for (int nt : nts) {
                 if (forced && forced->threads && nt != forced->threads) continue;
                 // thread-private hot words + the CTA's cold words, for every
@@ -260,10 +284,7 @@ static int choose_config(vr_agg* h, const vr_tune_choice* forced) {
     SmemMap m = smem_map(c.stages, stage_bytes_for(P, c.tile_rows), tier_bytes);
     // blocks per SM: shared memory and registers (the ahead-of-time kernel's;
     // refined once a per-spec kernel is loaded)
-    c.blocks_per_sm = di.fits(2, m.total) ? 2 : 1;
-    int regs = aggregate_kernel_regs(P.kw, c.tier);
-    if (regs > 0 && 2 * ((regs + 7) / 8 * 8) * (c.threads + 32) > 65536) c.blocks_per_sm = 1;
-    if (forced && forced->blocks_per_sm) c.blocks_per_sm = forced->blocks_per_sm;
+    c.blocks_per_sm = ctas_per_sm(di, m.total, aggregate_kernel_regs(P.kw, c.tier), c.threads, wanted_ctas(forced));
     if (m.total > budget) return set_err(h, VR_ERR_UNSUPPORTED, "configuration exceeds shared memory");
     const bool jit_on = jit_enabled() && !(fl & VR_SPEC_NO_JIT) && !h->prebuilt_only;
     if (c.threads % 32 || c.threads > (jit_on ? kMaxConsumerThreadsJit : kMaxConsumerThreads) || c.tile_rows % 128)
@@ -408,15 +429,13 @@ int agg_build(const vr_agg_spec* spec, const vr_tune_choice* forced, vr_agg** ou
         shape.tier = h->cfg.tier;
         shape.rchunk = h->cfg.rchunk;
         shape.threads = h->cfg.threads;
-        // compiled for two CTAs per SM (registers capped to fit) when their
-        // shared memory fits and no choice forces one
-        const bool two = di.fits(2, h->launch.smem_bytes) && !(forced && forced->blocks_per_sm == 1);
-        shape.min_blocks = two ? 2 : 1;
+        // compiled for as many CTAs per SM as shared memory allows, up to the
+        // wanted count (registers capped to fit)
+        const int want = wanted_ctas(forced);
+        shape.min_blocks = ctas_per_sm(di, h->launch.smem_bytes, 0, h->cfg.threads, want);
         h->jit = jit_get(h->plan.prog, shape, h->device, &why);
         if (h->jit) {
-            int regs = jit_regs(h->jit);
-            int bps = di.fits(2, h->launch.smem_bytes) ? 2 : 1;
-            if (2 * ((regs + 7) / 8 * 8) * (h->cfg.threads + 32) > 65536) bps = 1;
+            const int bps = ctas_per_sm(di, h->launch.smem_bytes, jit_regs(h->jit), h->cfg.threads, want);
             h->cfg.blocks_per_sm = bps;
             h->blocks = di.sms * bps;
             h->stats.blocks = h->blocks;
