@@ -204,13 +204,27 @@ VR_DEV int64_t fast_value(const OpDesc& o, const V& v, int64_t r, bool& exact) {
             return in_valid(o, v, o.col, r) ? ld_int(v, o.col, o.lane, r) : 0;
         case OP_SUM_PROD: {
             const int64_t a = term_value(o, v, r, 0), b = term_value(o, v, r, 1);
-            int64_t p = a * b;
-            bool fits = __mul64hi(a, b) == (p >> 63);
-            if (o.nterms == 3) {
-                const int64_t c = term_value(o, v, r, 2);
-                const int64_t q = p * c;
-                fits = fits && __mul64hi(p, c) == (q >> 63);
-                p = q;
+            const int64_t c = o.nterms == 3 ? term_value(o, v, r, 2) : 1;
+            // factors within 32 bits (decimal(9, s) terms, and the values of
+            // most wider ones): widening 32-bit multiplies, exact in int64 when
+            // a three-factor product's first product also fits 32 bits. The
+            // whole warp takes one path (direct-tier chunks keep every lane).
+            const int64_t ab32 = (int64_t)(int32_t)a * (int32_t)b;
+            const bool small =
+                a == (int32_t)a && b == (int32_t)b && c == (int32_t)c && (o.nterms != 3 || ab32 == (int32_t)ab32);
+            int64_t p;
+            bool fits;
+            if (__all_sync(kFull, small)) {
+                p = o.nterms == 3 ? (int64_t)(int32_t)ab32 * (int32_t)c : ab32;
+                fits = true;
+            } else {
+                p = a * b;
+                fits = __mul64hi(a, b) == (p >> 63);
+                if (o.nterms == 3) {
+                    const int64_t q = p * c;
+                    fits = fits && __mul64hi(p, c) == (q >> 63);
+                    p = q;
+                }
             }
             exact = fits && within_precision64(p, o.prec) && terms_valid(o, v, r);
             return exact ? p : 0;
