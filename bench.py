@@ -48,7 +48,7 @@ def log(*a):
 # its group count, not the rows, so those figures hold only at the row count
 # they were captured at (profiles/aggregate_plain_1M.md,
 # profiles/aggregate_high_cardinality_100M.md).
-TRAFFIC_PER_ROW = {"decimal": (320.069632e6 + 4.935936e6) / 8_000_000}
+TRAFFIC_PER_ROW = {"decimal": (320.074496e6 + 4.034816e6) / 8_000_000}
 TRAFFIC_AT_ROWS = {"plain": (1 << 20, 25.473792e6 + 6.912e3), "highcard": (100_000_000, 7.71e9 + 2.57e9)}
 FLUSH_BYTES = 1 << 30  # written on the step's stream before each step's start event
 
@@ -498,7 +498,7 @@ def run_serving(args, device):
     rng = np.random.default_rng(G.SEEDS["serving"])
     fns = [A.CountAgg(), A.SumLongAgg(1), A.MinMaxAgg(1, True), A.MinMaxAgg(1, False), A.SumDoubleAgg(2),
            A.MinMaxAgg(2, True), A.MinMaxAgg(2, False)]
-    srv = vr.AggregateServer(device=device, slots=8, hbm_cap_bytes=120 << 30)
+    srv = vr.AggregateServer(device=device, slots=args.slots, hbm_cap_bytes=120 << 30)
     queries, pool, bufs = [], [], []
     max_rows = 1 << 20
     for q in range(16):
@@ -547,7 +547,8 @@ def run_serving(args, device):
                                f"{args.rate:g} requests/s for {args.seconds:g} s, batches of 4,096..1,048,576 "
                                "rows from pinned host memory", "hbm_cap_gb": 120},
         "serving": {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-                    "max_ms": float(lat.max()), "requests": n_req, "admitted_immediately": st.admitted_immediately,
+                    "max_ms": float(lat.max()), "p99_wait_ms": st.p99_wait_ms, "p99_service_ms": st.p99_service_ms,
+                    "requests": n_req, "slots": args.slots, "admitted_immediately": st.admitted_immediately,
                     "queued": st.queued, "rejected": st.rejected, "hbm_peak_gb": st.hbm_peak / 1e9,
                     "offered_rows_per_s": rows_done / float(np.sum(gaps))},
         "gpu_launches": int(st.completed),
@@ -615,6 +616,7 @@ def main():
     ap.add_argument("--instances", type=int, default=512, help="batched: instances")
     ap.add_argument("--rate", type=float, default=2000.0, help="serving: requests/s")
     ap.add_argument("--seconds", type=float, default=10.0, help="serving: trace length")
+    ap.add_argument("--slots", type=int, default=32, help="serving: requests in flight on the device")
     ap.add_argument("--rows", type=int, default=None)
     ap.add_argument("--chunk-rows", type=int, default=8 << 20)
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline sample length")

@@ -369,6 +369,8 @@ typedef struct vr_srv_stats {
     double mean_ms;
     int64_t hbm_in_use;
     int64_t hbm_peak;
+    double p99_wait_ms;        /* submit -> admitted to the device             */
+    double p99_service_ms;     /* admitted -> result ready                     */
 } vr_srv_stats;
 
 typedef struct vr_srv vr_srv;

@@ -34,6 +34,7 @@ struct Request {
     std::vector<vr_column> cols;
     int64_t bytes = 0;
     Clock::time_point t_submit;
+    Clock::time_point t_admit;
     Clock::time_point t_done;
     int state = 0;  // 0 queued, 1 running, 2 done
     int status = VR_OK;
@@ -58,6 +59,8 @@ struct vr_srv {
     std::map<uint64_t, std::shared_ptr<Request>> tickets;
     std::vector<Query> queries;
     std::vector<double> latencies_ms;
+    std::vector<double> waits_ms;     // submit -> admit
+    std::vector<double> services_ms;  // admit -> done
     int in_flight = 0;
     int64_t in_flight_bytes = 0;
     int64_t table_bytes = 0;
@@ -87,6 +90,8 @@ void CUDART_CB on_done(void* p) {
         s->queries[r.qid].in_flight--;
         double ms = std::chrono::duration<double, std::milli>(r.t_done - r.t_submit).count();
         s->latencies_ms.push_back(ms);
+        s->waits_ms.push_back(std::chrono::duration<double, std::milli>(r.t_admit - r.t_submit).count());
+        s->services_ms.push_back(std::chrono::duration<double, std::milli>(r.t_done - r.t_admit).count());
         s->st.completed++;
         s->st.rows += r.batch.num_rows;
         s->st.hbm_in_use = s->table_bytes + s->in_flight_bytes;
@@ -129,6 +134,7 @@ void dispatch_loop(vr_srv* s) {
             }
             s->queue.erase(it);
             r->state = 1;
+            r->t_admit = Clock::now();
             s->in_flight++;
             s->in_flight_bytes += r->bytes;
             q.in_flight++;
@@ -291,6 +297,8 @@ int vr_srv_get_stats(vr_srv* s, vr_srv_stats* st) {
     *st = s->st;
     st->p50_ms = percentile(s->latencies_ms, 0.50);
     st->p99_ms = percentile(s->latencies_ms, 0.99);
+    st->p99_wait_ms = percentile(s->waits_ms, 0.99);
+    st->p99_service_ms = percentile(s->services_ms, 0.99);
     double mx = 0, sum = 0;
     for (double v : s->latencies_ms) {
         mx = std::max(mx, v);

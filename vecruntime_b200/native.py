@@ -136,7 +136,8 @@ class SrvStats(C.Structure):
     _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("admitted_immediately", C.c_int64),
                 ("queued", C.c_int64), ("rejected", C.c_int64), ("rows", C.c_int64),
                 ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("max_ms", C.c_double),
-                ("mean_ms", C.c_double), ("hbm_in_use", C.c_int64), ("hbm_peak", C.c_int64)]
+                ("mean_ms", C.c_double), ("hbm_in_use", C.c_int64), ("hbm_peak", C.c_int64),
+                ("p99_wait_ms", C.c_double), ("p99_service_ms", C.c_double)]
 
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib", "libvrgpu.so")
