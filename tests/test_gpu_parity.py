@@ -181,3 +181,28 @@ def test_direct_tier_id_outside_its_dictionary_is_an_error(cuda):
         agg.sync()
     assert e.value.status == N.VR_ERR_INVALID
     agg.close()
+
+
+@pytest.mark.parametrize("flags", [0, N.VR_SPEC_FORCE_SHARED, N.VR_SPEC_FORCE_GLOBAL])
+@pytest.mark.parametrize("shape", ["shared_last_word", "zero_first_word"])
+def test_two_word_keys_under_concurrent_inserts(cuda, flags, shape):
+    """Composite int64 x int32 keys take two key words, claimed and published
+    by one 128-bit CAS and probed with plain 16-byte reads. Every CTA meets
+    the same new keys at once; keys that share their last word, or whose
+    first word is zero (so a stale zero word reads like part of the key),
+    drive the probe from the plain read into the CAS fallback."""
+    rng = np.random.default_rng(20261204)
+    n = 1 << 20
+    if shape == "shared_last_word":
+        k1 = rng.integers(0, 4096, size=n).astype(np.int64)
+        k2 = np.full(n, 3, np.int32)
+    else:
+        k1 = np.where(rng.random(n) < 0.5, 0, rng.integers(-50, 50, size=n)).astype(np.int64)
+        k2 = rng.integers(0, 64, size=n).astype(np.int32)
+    nulls = rng.random(n) < 0.02
+    v = rng.integers(-1000, 1000, size=n).astype(np.int64)
+    cols = [Cc.longs(k1, nulls), Cc.ints(k2, nullable=False), Cc.longs(v, nullable=False)]
+    fns = [A.CountAgg(), A.SumLongAgg(2), A.MinMaxAgg(2, True), A.MinMaxAgg(2, False)]
+    groups = len(set(zip(np.where(nulls, -1 << 62, k1).tolist(), k2.tolist())))
+    w = G.Workload("two_word_keys", cols, [0, 1], fns, groups, n)
+    check(w, batches_of(w, n // 4), flags=flags, device_batches=True)

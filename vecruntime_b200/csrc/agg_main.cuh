@@ -72,10 +72,11 @@ VR_DEV void producer_loop(const Program& P, const BatchDesc* __restrict__ descs,
     if (cfg.test_stall) return;  // test hook: nothing issued, nothing in flight
     int cur = -1;
     int64_t t_next = (int64_t)atomicAdd((unsigned long long*)tile_counter, 1ull);
-    for (int64_t k = 0;; ++k) {
-        int s = (int)(k % NS);
-        uint32_t parity = (uint32_t)((k / NS) & 1);
-        if (!mbar_wait(&empty[s], parity ^ 1u, (uint32_t)cfg.wait_polls)) {
+    // the stage index and its barrier phase advance with each tile (a 64-bit
+    // division by the run-time stage count per tile costs more than the tile's
+    // own bookkeeping)
+    for (int s = 0, parity = 0;; s = s + 1 == NS ? 0 : s + 1, parity ^= s == 0) {
+        if (!mbar_wait(&empty[s], (uint32_t)parity ^ 1u, (uint32_t)cfg.wait_polls)) {
             set_error(descs[0].ctrl, kErrTimeout);
             return;
         }
@@ -604,10 +605,9 @@ VR_DEV void aggregate_body(const BatchDesc* __restrict__ descs, const LaunchCfg&
     const int sslots = cfg.tier_bytes / (8 * VR_PSW(P));
     int cur = -1;
     uint32_t new_groups = 0;
-    for (int64_t k = 0;; ++k) {
-        int s = (int)(k % cfg.stages);
-        uint32_t parity = (uint32_t)((k / cfg.stages) & 1);
-        if (!mbar_wait(&full[s], parity, (uint32_t)cfg.wait_polls)) {
+    const int NS = cfg.stages;
+    for (int s = 0, parity = 0;; s = s + 1 == NS ? 0 : s + 1, parity ^= s == 0) {
+        if (!mbar_wait(&full[s], (uint32_t)parity, (uint32_t)cfg.wait_polls)) {
             set_error(descs[0].ctrl, kErrTimeout);
             break;
         }
