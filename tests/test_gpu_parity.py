@@ -82,6 +82,40 @@ def test_decimal_report_direct_tier(cuda):
     assert st.tier == 0
 
 
+@pytest.mark.parametrize("how", ["no_tma", "device", "device_unaligned"])
+def test_decimal_report_direct_tier_tile_paths(cuda, how):
+    """Direct-tier tiles are read from the stage in shared memory when the
+    producer bulk-copied them (full tiles of 16-byte aligned batches), and
+    from the batch's own buffers otherwise (the last partial tile, NO_TMA,
+    buffers that are not 16-byte aligned): every path against the oracle."""
+    import torch
+
+    w = G.decimal_report(rows=300_001)
+    if how == "no_tma":
+        check(w, [w.batch()], flags=N.VR_SPEC_NO_TMA)
+        return
+    if how == "device":
+        check(w, [w.batch()], device_batches=True)
+        return
+    # every column one element past a 256-byte aligned allocation: 4- and
+    # 8-byte aligned, never 16-byte aligned
+    hb = w.batch()
+    keep, ptrs = [], []
+    for c in hb.columns:
+        t = torch.empty(c.data.nbytes + c.data.itemsize, dtype=torch.uint8, device="cuda")
+        t[c.data.itemsize:].copy_(torch.from_numpy(c.data.view(np.uint8)))
+        keep.append(t)
+        ptrs.append(t.data_ptr() + c.data.itemsize)
+    db = Cc.DeviceBatch(hb.num_rows, ptrs, [None] * len(ptrs))
+    agg = vr.GpuHashAggregate(w.columns, w.keys, w.functions, est_groups=w.est_groups, max_batch_rows=hb.num_rows)
+    agg.consume(db)
+    n = agg.num_groups()
+    out, types, st = agg.emit(), agg.output_types, agg.stats()
+    agg.close()
+    assert st.tier == 0
+    compare(w.spec(), types, out, n, *run_oracle(w, [hb]))
+
+
 def test_decimal_report_hash_tier(cuda):
     w = G.decimal_report(rows=300_000)
     check(w, [w.batch()], flags=N.VR_SPEC_FORCE_SHARED)

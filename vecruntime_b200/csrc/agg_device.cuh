@@ -394,11 +394,31 @@ VR_DEV int64_t ld_int(const TileView& v, int c, int lane, int64_t r) {
     return lane == VR_INT32 || lane == VR_DICT32 ? (int64_t)ld_i32(v, c, r) : ld_i64(v, c, r);
 }
 
+// Loads from a tile the producer staged in shared memory, by 32-bit shared
+// address (cheaper than a generic load, which must first find the address
+// space). Only for tiles the stage header marks as staged: a batch's last
+// partial tile, and batches whose buffers are not 16-byte aligned, are read
+// in place from global memory.
+VR_DEV int32_t lds32(const void* base, int64_t r) {
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(base) + (uint32_t)r * 4u;
+    int32_t x;
+    asm("ld.shared.s32 %0, [%1];" : "=r"(x) : "r"(a));
+    return x;
+}
+VR_DEV int64_t lds64(const void* base, int64_t r) {
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(base) + (uint32_t)r * 8u;
+    int64_t x;
+    asm("ld.shared.s64 %0, [%1];" : "=l"(x) : "r"(a));
+    return x;
+}
+
 // The columns one op reads, with their pointers in registers: built once per
 // op per chunk of rows, so the per-row loop reloads nothing from the tile
 // header after a store. Column c of the op is 0 (input / first factor),
-// 1 (second buffer / factor) or 2 (third factor).
-struct OpView {
+// 1 (second buffer / factor) or 2 (third factor). SM: the tile's data is
+// staged in shared memory (its validity bitmaps may still be global).
+template <bool SM>
+struct OpViewT {
     const char* d0;
     const char* d1;
     const char* d2;
@@ -406,30 +426,54 @@ struct OpView {
     const uint32_t* v1;
     const uint32_t* v2;
 };
+using OpView = OpViewT<false>;
 VR_DEV const char* vdata(const TileView& v, int c) { return v.data[c]; }
-VR_DEV const char* vdata(const OpView& v, int c) { return c == 0 ? v.d0 : c == 1 ? v.d1 : v.d2; }
-VR_DEV const uint32_t* vvalid(const OpView& v, int c) { return c == 0 ? v.v0 : c == 1 ? v.v1 : v.v2; }
-VR_DEV bool col_valid(const OpView& v, int c, int64_t r) {
+template <bool SM>
+VR_DEV const char* vdata(const OpViewT<SM>& v, int c) { return c == 0 ? v.d0 : c == 1 ? v.d1 : v.d2; }
+template <bool SM>
+VR_DEV const uint32_t* vvalid(const OpViewT<SM>& v, int c) { return c == 0 ? v.v0 : c == 1 ? v.v1 : v.v2; }
+template <bool SM>
+VR_DEV bool col_valid(const OpViewT<SM>& v, int c, int64_t r) {
     const uint32_t* w = vvalid(v, c);
     return w == nullptr || bit_at(w, r);
 }
-VR_DEV int32_t ld_i32(const OpView& v, int c, int64_t r) { return reinterpret_cast<const int32_t*>(vdata(v, c))[r]; }
-VR_DEV int64_t ld_i64(const OpView& v, int c, int64_t r) { return reinterpret_cast<const int64_t*>(vdata(v, c))[r]; }
-VR_DEV double ld_f64(const OpView& v, int c, int64_t r) { return reinterpret_cast<const double*>(vdata(v, c))[r]; }
-VR_DEV I128 ld_d128(const OpView& v, int c, int64_t r) {
-    const uint64_t* p = reinterpret_cast<const uint64_t*>(vdata(v, c)) + 2 * r;
+template <bool SM>
+VR_DEV int32_t ld_i32(const OpViewT<SM>& v, int c, int64_t r) {
+    if constexpr (SM) return lds32(vdata(v, c), r);
+    return reinterpret_cast<const int32_t*>(vdata(v, c))[r];
+}
+template <bool SM>
+VR_DEV int64_t ld_i64(const OpViewT<SM>& v, int c, int64_t r) {
+    if constexpr (SM) return lds64(vdata(v, c), r);
+    return reinterpret_cast<const int64_t*>(vdata(v, c))[r];
+}
+template <bool SM>
+VR_DEV double ld_f64(const OpViewT<SM>& v, int c, int64_t r) {
+    if constexpr (SM) return __longlong_as_double((long long)lds64(vdata(v, c), r));
+    return reinterpret_cast<const double*>(vdata(v, c))[r];
+}
+template <bool SM>
+VR_DEV I128 ld_d128(const OpViewT<SM>& v, int c, int64_t r) {
     I128 x;
-    x.lo = p[0];
-    x.hi = (int64_t)p[1];
+    if constexpr (SM) {
+        x.lo = (uint64_t)lds64(vdata(v, c), 2 * r);
+        x.hi = lds64(vdata(v, c), 2 * r + 1);
+    } else {
+        const uint64_t* p = reinterpret_cast<const uint64_t*>(vdata(v, c)) + 2 * r;
+        x.lo = p[0];
+        x.hi = (int64_t)p[1];
+    }
     return x;
 }
-VR_DEV int64_t ld_int(const OpView& v, int c, int lane, int64_t r) {
+template <bool SM>
+VR_DEV int64_t ld_int(const OpViewT<SM>& v, int c, int lane, int64_t r) {
     return lane == VR_INT32 || lane == VR_DICT32 ? (int64_t)ld_i32(v, c, r) : ld_i64(v, c, r);
 }
 
 // The op's columns from a tile view; `oo` is `o` with its column indices
 // renumbered to the view's 0..2.
-VR_DEV void make_opview(const OpDesc& o, const TileView& v, OpDesc& oo, OpView& ov) {
+template <bool SM>
+VR_DEV void make_opview(const OpDesc& o, const TileView& v, OpDesc& oo, OpViewT<SM>& ov) {
     oo = o;
     ov.d0 = ov.d1 = ov.d2 = nullptr;
     ov.v0 = ov.v1 = ov.v2 = nullptr;
@@ -525,6 +569,7 @@ VR_DEV void pack_key(const Program& P, const TileView& v, int64_t r, uint64_t (&
 
 // Direct tier: one field's share of the combination index; -1 when its id
 // lies outside the declared dictionary (null is the field's last value).
+template <bool SM = false>
 VR_DEV int64_t direct_field(const KeyField& kf, const TileView& v, int64_t r) {
     int64_t val;
     if (kf.null_word >= 0 && !col_valid(v, kf.col, r)) {  // only nullable keys carry a bitmap
@@ -532,7 +577,7 @@ VR_DEV int64_t direct_field(const KeyField& kf, const TileView& v, int64_t r) {
     } else if (kf.lane == VR_BOOL) {
         val = bit_at(reinterpret_cast<const uint32_t*>(v.data[kf.col]), r);
     } else {
-        val = (int64_t)(uint32_t)ld_i32(v, kf.col, r);
+        val = (int64_t)(uint32_t)(SM ? lds32(v.data[kf.col], r) : ld_i32(v, kf.col, r));
         if (val >= (int64_t)kf.card - (kf.null_word >= 0 ? 1 : 0)) return -1;
     }
     return val * kf.mul;
