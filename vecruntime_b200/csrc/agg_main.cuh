@@ -256,6 +256,42 @@ VR_DEV void direct_op(const OpDesc& op, const TileView& v, const int64_t (&r)[R]
     uint64_t* hot = priv + (size_t)o.hword * nt + ctid;
     uint64_t* cop = cold + o.word;
     const size_t gstride = (size_t)hw * nt;
+    if constexpr (K == OP_SUM_PROD) {
+        // The chunk's products when every factor of the warp's R rows fits 32
+        // bits (one vote for the chunk): widening multiplies, and no per-row
+        // exactness bookkeeping (measured: 0.650 against 0.674 ms per 60M
+        // decimal-report rows). Otherwise the per-row path below.
+        int64_t p[R];
+        bool small = true;
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+            const int64_t a = term_value(o, ov, r[j], 0), b = term_value(o, ov, r[j], 1);
+            const int64_t c = o.nterms == 3 ? term_value(o, ov, r[j], 2) : 1;
+            const int64_t ab32 = (int64_t)(int32_t)a * (int32_t)b;
+            small = small && a == (int32_t)a && b == (int32_t)b && c == (int32_t)c &&
+                    (o.nterms != 3 || ab32 == (int32_t)ab32);
+            p[j] = o.nterms == 3 ? (int64_t)(int32_t)ab32 * (int32_t)c : ab32;
+            small = small && within_precision64(p[j], o.prec) && terms_valid(o, ov, r[j]);
+        }
+        if (__all_sync(kFull, small)) {
+            uint32_t wrap = 0;
+#pragma unroll
+            for (int j = 0; j < R; ++j) {
+                uint64_t* h = hot + g[j] * gstride;
+                const int64_t s = (int64_t)*h;
+                const int64_t ns = (int64_t)((uint64_t)s + (uint64_t)p[j]);
+                *h = (uint64_t)ns;
+                wrap |= (uint32_t)(((s ^ ns) & (p[j] ^ ns)) < 0) << j;
+            }
+            if (wrap) {
+#pragma unroll
+                for (int j = 0; j < R; ++j)
+                    if ((wrap >> j) & 1u)  // +-2^64 into the carry-save high word (+-2^32 there)
+                        s_add(cop + (size_t)g[j] * aw + 1, p[j] > 0 ? (1ull << 32) : (0ull - (1ull << 32)));
+            }
+            return;
+        }
+    }
     if constexpr (OneAdd<K>::value) {
         constexpr bool kWraps = K == OP_SUM_I64 || K == OP_SUM_PROD;
         uint32_t rare = 0, wrap = 0;
