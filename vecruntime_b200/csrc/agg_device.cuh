@@ -583,6 +583,22 @@ VR_DEV int64_t direct_field(const KeyField& kf, const TileView& v, int64_t r) {
     return val * kf.mul;
 }
 
+// direct_field in 32-bit arithmetic (a combination index is below 65,536).
+template <bool SM>
+VR_DEV int direct_field32(const KeyField& kf, const TileView& v, int64_t r) {
+    int val;
+    if (kf.null_word >= 0 && !col_valid(v, kf.col, r)) {
+        val = (int)kf.card - 1;
+    } else if (kf.lane == VR_BOOL) {
+        val = (int)bit_at(reinterpret_cast<const uint32_t*>(v.data[kf.col]), r);
+    } else {
+        const uint32_t id = (uint32_t)(SM ? lds32(v.data[kf.col], r) : ld_i32(v, kf.col, r));
+        if (id >= (uint32_t)kf.card - (kf.null_word >= 0 ? 1u : 0u)) return -1;
+        val = (int)id;
+    }
+    return val * (int)kf.mul;
+}
+
 // Direct tier: the combination index of a row's dictionary / boolean keys;
 // -1 when an id lies outside its declared dictionary.
 VR_DEV int64_t direct_index(const Program& P, const TileView& v, int64_t r) {

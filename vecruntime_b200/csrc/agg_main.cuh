@@ -334,7 +334,7 @@ VR_DEV void direct_op(const OpDesc& op, const TileView& v, const int64_t (&r)[R]
 template <class F>
 VR_DEV void jit_for_op(int i, F&& f);
 template <bool SM>
-VR_DEV int64_t jit_direct_index(const TileView& v, int64_t r);
+VR_DEV int jit_direct_index(const TileView& v, int64_t r);
 template <int KW>
 VR_DEV void jit_pack_key(const TileView& v, int64_t r, uint64_t (&k)[KW], bool& side, bool& bad);
 #define VR_NUM_OPS(P) VR_JIT_NUM_OPS
@@ -467,11 +467,12 @@ VR_DEV void direct_chunk(const Program& P, const BatchDesc& D, const TileView& v
 #pragma unroll
     for (int j = 0; j < R; ++j) {
 #ifdef VR_JIT
-        const int64_t gi = jit_direct_index<SM>(v, r[j]);
+        const int gi = jit_direct_index<SM>(v, r[j]);
+        const bool ok = (unsigned)gi < (unsigned)VR_PDSLOTS(P);
 #else
         const int64_t gi = direct_index(P, v, r[j]);
-#endif
         const bool ok = gi >= 0 && gi < VR_PDSLOTS(P);
+#endif
         bad |= (uint32_t)(live[j] && !ok) << j;
         // rows that do not count accumulate into the trash group (never flushed)
         g[j] = live[j] && ok ? (int)gi : (int)VR_PDSLOTS(P);
@@ -578,7 +579,7 @@ VR_DEV void direct_tile(const Program& P, const BatchDesc& D, const TileView& v,
         bool live[R];
 #pragma unroll
         for (int j = 0; j < R; ++j) {
-            const int64_t rr = base + j * NT + ctid;
+            const int rr = base + j * NT + ctid;
             live[j] = rr < rows && (v.sel == nullptr || bit_at(v.sel, rr));
             r[j] = rr < rows ? rr : rows - 1;  // past the tile: a real row, counted into the trash group
         }

@@ -185,10 +185,10 @@ std::string op_literal(const OpDesc& d) {
 std::string hooks(const Program& P) {
     std::ostringstream o;
     o << "namespace vr {\n";
-    o << "template <bool SM>\nVR_DEV int64_t jit_direct_index(const TileView& v, int64_t r) {\n  int64_t idx = 0;\n";
+    o << "template <bool SM>\nVR_DEV int jit_direct_index(const TileView& v, int64_t r) {\n  int idx = 0;\n";
     for (int f = 0; f < P.num_keys; ++f)
         o << "  { constexpr KeyField kf = " << key_literal(P.keys[f])
-          << "; int64_t x = direct_field<SM>(kf, v, r); if (x < 0) return -1; idx += x; }\n";
+          << "; int x = direct_field32<SM>(kf, v, r); if (x < 0) return -1; idx += x; }\n";
     o << "  return idx;\n}\n";
     o << "template <int KW>\nVR_DEV void jit_pack_key(const TileView& v, int64_t r, uint64_t (&k)[KW], bool& side, "
          "bool& bad) {\n#pragma unroll\n  for (int i = 0; i < KW; ++i) k[i] = 0;\n  side = false;\n  bad = false;\n";
