@@ -346,6 +346,18 @@ static int alloc_slot(vr_agg* h, StageSlot& s) {
     return VR_OK;
 }
 
+// Device staging for a host batch of n rows: every staged column and
+// validity bitmap, plus the selection bitmap, each 256-byte aligned.
+static size_t staging_bytes(const Program& P, int64_t n) {
+    size_t need = 0;
+    for (int c = 0; c < P.num_cols; ++c) {
+        int w = P.col_width[c];
+        need += al256(w ? (size_t)n * w : (size_t)(n + 7) / 8 + 4);
+        need += al256((size_t)(n + 7) / 8 + 4);
+    }
+    return need + al256((size_t)(n + 7) / 8 + 4);
+}
+
 static int ensure_deferred(vr_agg* h, StageSlot& s, int64_t rows) {
     if (h->cfg.tier == kTierDirect || s.deferred_cap >= rows) return VR_OK;
     cudaFree(s.deferred);
@@ -356,6 +368,31 @@ static int ensure_deferred(vr_agg* h, StageSlot& s, int64_t rows) {
     if (e == cudaSuccess) e = cudaMalloc(&s.deferred_tmp, (size_t)cap * 8);
     if (e != cudaSuccess) return cuda_err(h, e, "deferred list");
     s.deferred_cap = cap;
+    return VR_OK;
+}
+
+// Sizes both staging sets (host batches) and deferred-row lists for batches
+// of up to `rows` rows now, so that no later update has to grow them: growing
+// means cudaFree, which waits for the whole device, and a server issuing many
+// queries' updates from one thread would stall on it.
+int agg_reserve(vr_agg* h, int64_t rows) {
+    if (rows <= 0) return VR_OK;
+    cudaSetDevice(h->device);
+    const size_t need = staging_bytes(h->plan.prog, rows);
+    for (StageSlot& s : h->slot) {
+        int rc = ensure_deferred(h, s, rows);
+        if (rc != VR_OK) return rc;
+        if (need <= s.dev_cap) continue;
+        if (s.dev) {
+            cudaError_t e = cudaFree(s.dev);
+            if (e != cudaSuccess) return cuda_err(h, e, "staging free");
+        }
+        s.dev = nullptr;
+        s.dev_cap = 0;
+        cudaError_t e = cudaMalloc(&s.dev, need);
+        if (e != cudaSuccess) return cuda_err(h, e, "staging allocation");
+        s.dev_cap = need;
+    }
     return VR_OK;
 }
 
@@ -513,13 +550,7 @@ static int stage_batch(vr_agg* h, StageSlot& s, const vr_batch& b, const char** 
         return VR_OK;
     }
     // host batch: one H2D copy per buffer into the slot's staging area
-    size_t need = 0;
-    for (int c = 0; c < P.num_cols; ++c) {
-        int w = P.col_width[c];
-        need += al256(w ? (size_t)n * w : (size_t)(n + 7) / 8 + 4);
-        need += al256((size_t)(n + 7) / 8 + 4);
-    }
-    need += al256((size_t)(n + 7) / 8 + 4);
+    const size_t need = staging_bytes(P, n);
     if (need > s.dev_cap) {
         if (s.dev) {
             cudaError_t e = cudaFree(s.dev);

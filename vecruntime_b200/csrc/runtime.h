@@ -129,6 +129,8 @@ int agg_build(const vr_agg_spec* spec, const vr_tune_choice* forced, vr_agg** ou
 // Fills a BatchDesc for a device-resident batch (no copies).
 void fill_desc(vr_agg* h, const vr_batch& b, BatchDesc& d, uint64_t* ctrl, const StageSlot& s, int64_t tile_begin);
 int agg_resolve_all(vr_agg* h);
+// Staging and deferred-row lists sized now for batches of up to `rows` rows.
+int agg_reserve(vr_agg* h, int64_t rows);
 cudaError_t agg_launch(vr_agg* h, const BatchDesc* descs, const LaunchCfg& L, int blocks, uint64_t* tile_counter,
                        cudaStream_t st);
 int64_t tiles_for(const vr_agg* h, int64_t rows);

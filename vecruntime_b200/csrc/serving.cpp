@@ -199,7 +199,15 @@ int vr_srv_open_query(vr_srv* s, const vr_agg_spec* spec, int32_t* query_id) {
     vr_agg* h = nullptr;
     int rc = vr_agg_create(spec, &h);
     if (rc != VR_OK) return rc;
+    // requests arrive from host memory at up to max_batch_rows rows: size the
+    // staging now, so the dispatcher never frees and reallocates it (cudaFree
+    // would stall every query's pipeline)
+    if ((rc = vr::agg_reserve(h, spec->max_batch_rows)) != VR_OK) {
+        vr_agg_destroy(h);
+        return rc;
+    }
     int64_t tb = h->table_slots * h->plan.prog.sw * 8;
+    for (const vr::StageSlot& sl : h->slot) tb += (int64_t)sl.dev_cap + sl.deferred_cap * 16;
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->table_bytes + tb > s->cfg.hbm_cap_bytes) {
         vr_agg_destroy(h);
