@@ -282,11 +282,7 @@ def run_ours(args, rank, world, device):
     st1 = agg.stats()
     kernel_ms = (st1.total_kernel_ms - kms0) / args.steps
     launches = st1.kernel_launches - launches0
-    total_ms = sum(step_ms)
-    total_ms = dist_max(total_ms, world, device)
-    ms_per_step = total_ms / args.steps
-    rows_total = w.rows * world
-    value = rows_total / (ms_per_step * 1e-3)
+    ms_per_step, value = weak_scaling(sum(step_ms), args.steps, w.rows, world, device)
 
     out_types = agg.output_types
     out_bytes = groups * output_row_bytes(out_types)
@@ -592,18 +588,27 @@ def dist_barrier(world):
 
 
 def dist_max(x, world, device):
+    """Max of x over the ranks (a CUDA tensor under NCCL, a CPU one under gloo)."""
     if world <= 1:
         return x
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device=torch.device("cuda", device))
+    where = torch.device("cuda", device) if dist.get_backend() == "nccl" else torch.device("cpu")
+    t = torch.tensor([x], dtype=torch.float64, device=where)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
 
 def dist_min(x, world, device):
     return -dist_max(-x, world, device)
+
+
+def weak_scaling(total_ms, steps, rows_per_rank, world, device):
+    """(ms per step, whole-job rows/s): every rank aggregates its own replica,
+    the job's time is the slowest rank's."""
+    ms_per_step = dist_max(total_ms, world, device) / steps
+    return ms_per_step, rows_per_rank * world / (ms_per_step * 1e-3)
 
 
 def main():
