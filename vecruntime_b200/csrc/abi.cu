@@ -249,21 +249,39 @@ static int choose_config(vr_agg* h, const vr_tune_choice* forced) {
                 }
             }
         }
-        // 2) otherwise two CTAs per SM with 1024-row tiles and a small hot-key
-        //    cache in front of HBM (the first keys a CTA meets hold it; under
-        //    skew those are the frequent ones). Measured on 20M Zipf(1.1) rows
-        //    with 4.2M groups: 3.3 ms against 4.4 ms for one CTA with 2048
-        //    slots and 4.9 ms without a cache.
+        // 2) otherwise two CTAs per SM with a hot-key cache in front of HBM
+        //    (the first keys a CTA meets hold it; under skew those are the
+        //    frequent ones). A bigger cache catches more of them but every
+        //    CTA flushes all of it into HBM at the end, a fixed cost per
+        //    launch (measured: 1,024 slots cost 33 us more than 256 on
+        //    uniform keys), so the cache grows with the batch: 256 slots
+        //    below 8M rows, 512 below 16M, then as many as two CTAs per SM
+        //    leave room for; the tile is the longest that still fits it.
+        //    Measured on Zipf(1.1) composite keys, 80-byte slots: 256-row
+        //    tiles with 1,024 slots 2.45 ms per 20M rows (12.9 per 100M),
+        //    512 x 512 2.64, 1024 x 256 2.86 (15.1), no cache 4.07.
         if (!done) {
-            c.tile_rows = forced && forced->tile_rows ? forced->tile_rows : 1024;
+            const int half = std::min(budget, di.smem_per_sm / 2 - di.smem_reserved);
+            const int64_t rows = h->spec.max_batch_rows > 0 ? h->spec.max_batch_rows : (int64_t)1 << 20;
+            int64_t want = 256;
+            while (want < 4096 && want * 2 * 16384 <= rows) want *= 2;
+            want = std::min<int64_t>(want, need);
+            if (forced && forced->tile_rows) {
+                c.tile_rows = forced->tile_rows;
+            } else {
+                c.tile_rows = 1024;
+                while (c.tile_rows > 256 && fit(c.tile_rows, 3, half) < want) c.tile_rows /= 2;
+            }
             c.stages = 3;
             while (c.stages > 2 && !fits(c.stages, c.tile_rows, 0)) --c.stages;
             while (!fits(c.stages, c.tile_rows, 0) && c.tile_rows > 256) c.tile_rows /= 2;
-            int64_t slots = fit(c.tile_rows, c.stages, budget);
+            const int64_t slots = fit(c.tile_rows, c.stages, budget);
+            const int64_t slots2 = fit(c.tile_rows, c.stages, half);
             c.smem_slots = 0;
             if (use_cache && slots >= 64) {
-                int64_t want = forced && forced->smem_slots ? next_pow2(forced->smem_slots) : std::min<int64_t>(need, 256);
-                c.smem_slots = (int)std::min(slots, want);
+                int64_t take = forced && forced->smem_slots ? next_pow2(forced->smem_slots)
+                                                            : std::min<int64_t>(want, std::max<int64_t>(slots2, 64));
+                c.smem_slots = (int)std::min(slots, take);
                 // keys settle within two slots of home or not at all, so a miss
                 // (most rows once the cache is full) costs two probes
                 c.s_probes = 2;
