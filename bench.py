@@ -174,23 +174,29 @@ def device_batch(w, device):
     return db, tensors
 
 
+def pin(a, lib, bufs):
+    """A copy of array `a` in pinned host memory (vr_host_alloc); the
+    allocation is appended to `bufs` for vr_host_free."""
+    if a is None:
+        return None
+    a = np.ascontiguousarray(a)
+    p = C.c_void_p()
+    rc = lib.vr_host_alloc(max(a.nbytes, 16), C.byref(p))
+    assert rc == 0, "pinned allocation"
+    dst = np.ctypeslib.as_array((C.c_uint8 * a.nbytes).from_address(p.value)).view(a.dtype).reshape(a.shape)
+    dst[...] = a
+    bufs.append(p)
+    return dst
+
+
 def pinned_copy(w, lib):
     """The workload's columns copied into pinned host memory (vr_host_alloc)."""
     from vecruntime_b200 import columns as Cc
 
     bufs = []
 
-    def pin(a):
-        if a is None:
-            return None
-        a = np.ascontiguousarray(a)
-        p = C.c_void_p()
-        rc = lib.vr_host_alloc(max(a.nbytes, 16), C.byref(p))
-        assert rc == 0, "pinned allocation"
-        dst = np.ctypeslib.as_array((C.c_uint8 * a.nbytes).from_address(p.value)).view(a.dtype).reshape(a.shape)
-        dst[...] = a
-        bufs.append(p)
-        return dst
+    def pin(a, pin=pin):
+        return pin(a, lib, bufs)
 
     cols = []
     for c in w.columns:
@@ -369,6 +375,11 @@ def run_e2e(args, w, lib, device, out_types):
     in_bytes = G.input_bytes(w)
     d2h = 0
     times = []
+    from vecruntime_b200 import aggregate as A
+
+    # the groups come back into pinned buffers allocated once (the first
+    # warm-up step sizes them), as a caller with a pinned output pool would
+    out_pinned, out_bufs = None, []
     for it in range(args.warmup + args.steps):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
@@ -376,14 +387,16 @@ def run_e2e(args, w, lib, device, out_types):
         for hb in bl:
             agg.consume(hb)
         groups = agg.num_groups()
-        out = agg.emit()
+        out = agg.emit(out=out_pinned) if out_pinned is not None else agg.emit()
         b.record(stream)
         torch.cuda.synchronize(device)
         if it >= args.warmup:
             times.append(a.elapsed_time(b))
         d2h = sum(d.nbytes + v.nbytes for d, v in out)
+        if out_pinned is None:
+            out_pinned = [(pin(d, lib, out_bufs), pin(v, lib, out_bufs)) for d, v in out]
     agg.close()
-    for p in bufs:
+    for p in bufs + out_bufs:
         lib.vr_host_free(p)
     ms = float(np.mean(times))
     return {"value": w.rows / (ms * 1e-3), "unit": "rows/s", "h2d_bytes_per_step": in_bytes,

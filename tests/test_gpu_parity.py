@@ -240,3 +240,44 @@ def test_two_word_keys_under_concurrent_inserts(cuda, flags, shape):
     groups = len(set(zip(np.where(nulls, -1 << 62, k1).tolist(), k2.tolist())))
     w = G.Workload("two_word_keys", cols, [0, 1], fns, groups, n)
     check(w, batches_of(w, n // 4), flags=flags, device_batches=True)
+
+
+def test_emit_into_caller_buffers(cuda):
+    """vr_agg_emit into caller-owned host buffers reused across calls (pinned
+    here, as a caller with a pinned output pool would pass): the same
+    groups as freshly allocated outputs, and a buffer too small for the
+    range is refused before anything is written."""
+    import ctypes as C
+
+    w = G.high_cardinality(rows=200_000, domain=50_000)
+    lib = N.lib()
+    agg = vr.GpuHashAggregate(w.columns, w.keys, w.functions, est_groups=w.est_groups, max_batch_rows=w.rows)
+    agg.consume(w.batch())
+    n = agg.num_groups()
+    fresh = agg.emit()
+    bufs = []
+
+    def pinned(a):
+        p = C.c_void_p()
+        assert lib.vr_host_alloc(max(a.nbytes, 16), C.byref(p)) == 0
+        bufs.append(p)
+        return np.ctypeslib.as_array((C.c_uint8 * a.nbytes).from_address(p.value)).view(a.dtype).reshape(a.shape)
+
+    try:
+        out = [(pinned(d), pinned(v)) for d, v in fresh]
+        for _ in range(2):
+            got = agg.emit(out=out)
+            for (d0, v0), (d1, v1) in zip(fresh, got):
+                assert np.array_equal(d0.view(np.uint8), d1.view(np.uint8))
+                assert np.array_equal(v0, v1)
+        half = n // 2
+        part = agg.emit(0, half, out=out)
+        assert np.array_equal(part[0][0][:half], fresh[0][0][:half])
+        small = [(d[:1], v[:1]) for d, v in out]
+        with pytest.raises(ValueError):
+            agg.emit(out=small)
+        compare(w.spec(), agg.output_types, fresh, n, *run_oracle(w, [w.batch()]))
+    finally:
+        agg.close()
+        for p in bufs:
+            lib.vr_host_free(p)

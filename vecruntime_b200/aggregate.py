@@ -144,6 +144,17 @@ class Spec:
         return rc, info, [outs[i] for i in range(info.num_outputs)]
 
 
+def _out_bytes(t: N.ColumnType, n: int) -> int:
+    """Bytes of an output column's data for n groups."""
+    if t.lane in (N.VR_INT32, N.VR_DICT32):
+        return 4 * n
+    if t.lane in (N.VR_INT64, N.VR_FLOAT64):
+        return 8 * n
+    if t.lane == N.VR_DECIMAL128:
+        return 16 * n
+    return max((n + 7) // 8, 1)  # BOOL: a bitmap
+
+
 def _out_arrays(t: N.ColumnType, n: int):
     nb = (n + 7) // 8
     if t.lane in (N.VR_INT32, N.VR_DICT32):
@@ -198,12 +209,23 @@ class GpuHashAggregate:
         self._pending.clear()
         return g.value
 
-    def emit(self, start: int = 0, end: Optional[int] = None):
-        """Groups [start, end) as a list of (data, validity) numpy pairs, one per output column."""
+    def emit(self, start: int = 0, end: Optional[int] = None, out=None):
+        """Groups [start, end) as a list of (data, validity) numpy pairs, one per
+        output column. `out`: such pairs to write into instead of new arrays
+        (e.g. views of pinned memory, reused batch after batch); each buffer
+        must hold the range."""
         total = self.num_groups()
         end = total if end is None else end
         n = end - start
-        arrays = [_out_arrays(t, n) for t in self.output_types]
+        if out is None:
+            arrays = [_out_arrays(t, n) for t in self.output_types]
+        else:
+            arrays = list(out)
+            if len(arrays) != len(self.output_types):
+                raise ValueError("emit: one (data, validity) pair per output column")
+            for t, (d, v) in zip(self.output_types, arrays):
+                if d.nbytes < _out_bytes(t, n) or v.nbytes < max((n + 7) // 8, 1):
+                    raise ValueError("emit: an output buffer is smaller than the range")
         outs = (N.OutColumn * max(1, len(arrays)))()
         for i, (d, v) in enumerate(arrays):
             outs[i].data = d.ctypes.data
