@@ -195,12 +195,12 @@ def pinned_copy(w, lib):
 
     bufs = []
 
-    def pin(a, pin=pin):
+    def pin_one(a):
         return pin(a, lib, bufs)
 
     cols = []
     for c in w.columns:
-        n = Cc.Col(c.lane, pin(c.data), pin(c.validity), c.precision, c.scale, c.dict_size, c.nullable)
+        n = Cc.Col(c.lane, pin_one(c.data), pin_one(c.validity), c.precision, c.scale, c.dict_size, c.nullable)
         if c.lane == 4:
             n._n = c._n
         cols.append(n)
