@@ -116,6 +116,17 @@ def test_decimal_report_direct_tier_tile_paths(cuda, how):
     compare(w.spec(), types, out, n, *run_oracle(w, [hb]))
 
 
+@pytest.mark.parametrize("threads,tile,ctas", [(96, 384, 3), (64, 256, 4), (160, 640, 2)])
+def test_decimal_report_direct_tier_block_shapes(cuda, threads, tile, ctas):
+    """A tuning choice may put up to four CTAs on an SM: each direct-tier
+    block shape gives the oracle's groups."""
+    t = N.TuneChoice()
+    t.tier, t.threads, t.tile_rows, t.blocks_per_sm = 0, threads, tile, ctas
+    w = G.decimal_report(rows=200_003)
+    st = check(w, [w.batch()], tune=t)
+    assert st.tier == 0 and st.tile_rows == tile and st.blocks == 148 * ctas
+
+
 def test_decimal_report_hash_tier(cuda):
     w = G.decimal_report(rows=300_000)
     check(w, [w.batch()], flags=N.VR_SPEC_FORCE_SHARED)
