@@ -128,6 +128,33 @@ def test_decimal_products_leave_the_fast_path(cuda, direct, checked):
     assert status == (N.VR_ERR_DECIMAL_PRECISION if checked else N.VR_OK)
 
 
+@pytest.mark.parametrize("direct", [False, True])
+def test_three_factor_product_reuses_the_two_factor_one(cuda, direct):
+    """sum(a*(1-b)) and sum(a*(1-b)*c) over the same a, b (the decimal
+    report's two product sums): the direct tier reuses the chunk's a*(1-b)
+    for the three-factor sum when every row of the chunk took the 32-bit
+    path. Row ranges where a*(1-b) leaves 32 bits (no reuse), where a factor
+    leaves 32 bits (the 64-bit path) and where factors are null meet the
+    oracle like the rest."""
+    rng = np.random.default_rng(11 + direct)
+    rows = 60_000
+    a = rng.integers(1, 10**6, rows, dtype=np.int64)
+    b = rng.integers(0, 11, rows, dtype=np.int64)
+    c = rng.integers(0, 9, rows, dtype=np.int64)
+    a[20_000:22_000] = rng.integers(10**8, 10**9, 2_000, dtype=np.int64)  # a*(1-b) past 32 bits
+    a[30_000:30_100] = rng.integers(10**12, 10**13, 100, dtype=np.int64)  # a factor past 32 bits
+    na = np.zeros(rows, bool)
+    na[40_000:41_000] = rng.random(1_000) < 0.5
+    k = keys(rng, rows, 16, direct)
+    cols = [k, Cc.decimals(a, 18, 2, na, nullable=True), Cc.decimals(b, 18, 2, nullable=False),
+            Cc.decimals(c, 18, 2, nullable=False)]
+    two = A.DecimalProduct([(1, 1, 0), (2, -1, 100)], precision=38)
+    three = A.DecimalProduct([(1, 1, 0), (2, -1, 100), (3, 1, 100)], precision=38)
+    fns = [A.WideDecimalSumAgg(two, 38, 4), A.WideDecimalSumAgg(three, 38, 6), A.CountAgg()]
+    w = G.Workload("prefix", cols, [0], fns, 16, rows)
+    assert same(w, [w.batch(0, 45_000), w.batch(45_000, rows)]) == N.VR_OK
+
+
 def merge_inputs(rng, rows, card, overflow=False):
     """Partial-aggregation buffers as a final aggregate receives them."""
     k = keys(rng, rows, card, False)

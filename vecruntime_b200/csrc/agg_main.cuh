@@ -247,9 +247,12 @@ VR_DEV int64_t fast_value(const OpDesc& o, const V& v, int64_t r, bool& exact) {
 // dictionary) arrive with the trash group, so the fast path has no branch per
 // row: one int64 add into the row's hot word, its signed wrap and any need
 // for the exact path noted in bit masks, handled after the chunk (rare).
+// `pre` / `pre_op`: the chunk's products of the last two-factor product op
+// (index pre_op, -1: none) that took the 32-bit path, for a three-factor op
+// that extends it by one factor (OpDesc::prefix_op).
 template <int K, int R, bool SM>
 VR_DEV void direct_op(const OpDesc& op, const TileView& v, const int64_t (&r)[R], const int (&g)[R], uint64_t* priv,
-                      uint64_t* cold, int nt, int ctid, int hw, int aw) {
+                      uint64_t* cold, int nt, int ctid, int hw, int aw, int opi, int64_t (&pre)[R], int& pre_op) {
     OpDesc o;
     OpViewT<SM> ov;
     make_opview(op, v, o, ov);
@@ -263,17 +266,33 @@ VR_DEV void direct_op(const OpDesc& op, const TileView& v, const int64_t (&r)[R]
         // decimal-report rows). Otherwise the per-row path below.
         int64_t p[R];
         bool small = true;
+        if (o.nterms == 3 && o.prefix_op > 0 && pre_op == o.prefix_op - 1) {
+            // the first two factors' product: the earlier op's, this chunk
 #pragma unroll
-        for (int j = 0; j < R; ++j) {
-            const int64_t a = term_value(o, ov, r[j], 0), b = term_value(o, ov, r[j], 1);
-            const int64_t c = o.nterms == 3 ? term_value(o, ov, r[j], 2) : 1;
-            const int64_t ab32 = (int64_t)(int32_t)a * (int32_t)b;
-            small = small && a == (int32_t)a && b == (int32_t)b && c == (int32_t)c &&
-                    (o.nterms != 3 || ab32 == (int32_t)ab32);
-            p[j] = o.nterms == 3 ? (int64_t)(int32_t)ab32 * (int32_t)c : ab32;
-            small = small && within_precision64(p[j], o.prec) && terms_valid(o, ov, r[j]);
+            for (int j = 0; j < R; ++j) {
+                const int64_t c = term_value(o, ov, r[j], 2);
+                small = small && pre[j] == (int32_t)pre[j] && c == (int32_t)c;
+                p[j] = (int64_t)(int32_t)pre[j] * (int32_t)c;
+                small = small && within_precision64(p[j], o.prec) && terms_valid(o, ov, r[j]);
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < R; ++j) {
+                const int64_t a = term_value(o, ov, r[j], 0), b = term_value(o, ov, r[j], 1);
+                const int64_t c = o.nterms == 3 ? term_value(o, ov, r[j], 2) : 1;
+                const int64_t ab32 = (int64_t)(int32_t)a * (int32_t)b;
+                small = small && a == (int32_t)a && b == (int32_t)b && c == (int32_t)c &&
+                        (o.nterms != 3 || ab32 == (int32_t)ab32);
+                p[j] = o.nterms == 3 ? (int64_t)(int32_t)ab32 * (int32_t)c : ab32;
+                small = small && within_precision64(p[j], o.prec) && terms_valid(o, ov, r[j]);
+            }
         }
         if (__all_sync(kFull, small)) {
+            if (o.nterms == 2) {
+#pragma unroll
+                for (int j = 0; j < R; ++j) pre[j] = p[j];
+                pre_op = opi;
+            }
             uint32_t wrap = 0;
 #pragma unroll
             for (int j = 0; j < R; ++j) {
@@ -479,10 +498,12 @@ VR_DEV void direct_chunk(const Program& P, const BatchDesc& D, const TileView& v
     }
     if (bad) set_error(D.ctrl, kErrBadKey);
     const int hw = VR_PHW(P), aw = VR_PAW(P);
+    int64_t pre[R];
+    int pre_op = -1;
     VR_UNROLL
     for (int i = 0; i < VR_NUM_OPS(P); ++i)
         for_op(P, i, [&](const OpDesc& op, auto tag) {
-            direct_op<decltype(tag)::value, R, SM>(op, v, r, g, priv, cold, nt, ctid, hw, aw);
+            direct_op<decltype(tag)::value, R, SM>(op, v, r, g, priv, cold, nt, ctid, hw, aw, i, pre, pre_op);
         });
 }
 

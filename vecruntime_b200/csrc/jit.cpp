@@ -152,7 +152,7 @@ std::string program_literal(const Program& P) {
         o << "{" << (int)d.kind << "," << (int)d.lane << "," << (int)d.flags << "," << (int)d.nwords << ","
           << (int)d.col << "," << (int)d.col2 << "," << (int)d.nterms << "," << (int)d.prec << "," << d.word << ","
           << d.hword << ",{" << (int)d.term_col[0] << "," << (int)d.term_col[1] << "," << (int)d.term_col[2] << "},{"
-          << (int)d.term_sign[0] << "," << (int)d.term_sign[1] << "," << (int)d.term_sign[2] << "}," << d.pad2 << ",{"
+          << (int)d.term_sign[0] << "," << (int)d.term_sign[1] << "," << (int)d.term_sign[2] << "}," << d.prefix_op << ",{"
           << (long long)d.term_add[0] << "LL," << (long long)d.term_add[1] << "LL," << (long long)d.term_add[2]
           << "LL}}" << (i + 1 < kMaxOps ? "," : "");
     }
@@ -175,7 +175,7 @@ std::string op_literal(const OpDesc& d) {
     o << "{" << (int)d.kind << "," << (int)d.lane << "," << (int)d.flags << "," << (int)d.nwords << "," << (int)d.col
       << "," << (int)d.col2 << "," << (int)d.nterms << "," << (int)d.prec << "," << d.word << "," << d.hword << ",{"
       << (int)d.term_col[0] << "," << (int)d.term_col[1] << "," << (int)d.term_col[2] << "},{" << (int)d.term_sign[0]
-      << "," << (int)d.term_sign[1] << "," << (int)d.term_sign[2] << "}," << d.pad2 << ",{" << (long long)d.term_add[0]
+      << "," << (int)d.term_sign[1] << "," << (int)d.term_sign[2] << "}," << d.prefix_op << ",{" << (long long)d.term_add[0]
       << "LL," << (long long)d.term_add[1] << "LL," << (long long)d.term_add[2] << "LL}}";
     return o.str();
 }

@@ -486,6 +486,21 @@ struct Builder {
         if (P.num_cols > kMaxCols) return fail(VR_ERR_UNSUPPORTED, "too many input columns");
         P.aw = words;
         P.sw = (P.kw + P.aw + 1) & ~1;
+        // a three-factor product whose first two factors are an earlier
+        // two-factor product's: the direct tier reuses that product
+        for (int i = 0; i < P.num_ops; ++i) {
+            OpDesc& b = P.ops[i];
+            if (b.kind != OP_SUM_PROD || b.nterms != 3) continue;
+            for (int k = 0; k < i && !b.prefix_op; ++k) {
+                const OpDesc& a = P.ops[k];
+                if (a.kind != OP_SUM_PROD || a.nterms != 2) continue;
+                bool same = true;
+                for (int t = 0; t < 2; ++t)
+                    same = same && a.term_col[t] == b.term_col[t] && a.term_sign[t] == b.term_sign[t] &&
+                           a.term_add[t] == b.term_add[t];
+                if (same) b.prefix_op = (int16_t)(k + 1);
+            }
+        }
         // direct tier: hot words per op (the running values every row touches)
         P.hw = 0;
         for (int i = 0; i < P.num_ops; ++i) {

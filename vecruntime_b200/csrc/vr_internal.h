@@ -73,7 +73,8 @@ struct OpDesc {
     int16_t hword;    // direct tier: first thread-private hot word
     int8_t term_col[3];
     int8_t term_sign[3];
-    int16_t pad2;
+    int16_t prefix_op;  // three-factor OP_SUM_PROD: 1 + index of an earlier two-factor
+                        // OP_SUM_PROD with the same first two factors; 0: none
     int64_t term_add[3];
 };
 
