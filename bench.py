@@ -48,7 +48,7 @@ def log(*a):
 # its group count, not the rows, so those figures hold only at the row count
 # they were captured at (profiles/aggregate_plain_1M.md,
 # profiles/aggregate_high_cardinality_100M.md).
-TRAFFIC_PER_ROW = {"decimal": (320.101632e6 + 3.906560e6) / 8_000_000}
+TRAFFIC_PER_ROW = {"decimal": (320.097792e6 + 4.176128e6) / 8_000_000}
 TRAFFIC_AT_ROWS = {"plain": (1 << 20, 25.473792e6 + 6.912e3), "highcard": (100_000_000, 7.72e9 + 2.57e9)}
 FLUSH_BYTES = 1 << 30  # written on the step's stream before each step's start event
 
