@@ -354,7 +354,6 @@ def run_e2e(args, w, lib, device, out_types):
     import vecruntime_b200 as vr
     from vecruntime_b200 import columns as Cc
     from vecruntime_b200 import datagen as G
-    from vecruntime_b200 import native as N
 
     cols, bufs = pinned_copy(w, lib)
     chunk = min(w.rows, args.chunk_rows)
@@ -375,8 +374,6 @@ def run_e2e(args, w, lib, device, out_types):
     in_bytes = G.input_bytes(w)
     d2h = 0
     times = []
-    from vecruntime_b200 import aggregate as A
-
     # the groups come back into pinned buffers allocated once (the first
     # warm-up step sizes them), as a caller with a pinned output pool would
     out_pinned, out_bufs = None, []
@@ -496,8 +493,6 @@ def run_serving(args, device):
     4,096..1,048,576 rows, for args.seconds: p50/p99 latency (submit ->
     device completion) and rows/s. Request batches come from a pinned pool
     (4 per query) reused by the seeded trace."""
-    import threading as th
-
     import torch
 
     import vecruntime_b200 as vr

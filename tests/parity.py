@@ -9,7 +9,7 @@ an absolute floor of ATOL_SCALE times the sum of magnitudes in the group
 from __future__ import annotations
 
 import math
-from typing import List, Sequence
+from typing import List
 
 import numpy as np
 

@@ -4,7 +4,6 @@ issues any copy (VRGPU_TEST_STALL_PRODUCER) and a short poll budget
 (VRGPU_TEST_WAIT_POLLS), the consumers' waits run out, the kernel records
 the timeout and returns, the host reports VR_ERR_TIMEOUT for that handle,
 and the next handle on the same device runs normally."""
-import os
 import time
 
 import pytest

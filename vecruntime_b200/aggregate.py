@@ -10,8 +10,8 @@ VectorGroupedAggregateIterator (VectorHashAggregateExec.scala:463-1039):
 from __future__ import annotations
 
 import ctypes as C
-from dataclasses import dataclass, field
-from typing import List, Optional, Sequence, Tuple
+from dataclasses import dataclass
+from typing import Optional, Sequence, Tuple
 
 import numpy as np
 

@@ -8,7 +8,6 @@ BOOL bit-packed.
 """
 from __future__ import annotations
 
-import ctypes as C
 from dataclasses import dataclass, field
 from typing import List, Optional, Sequence
 

@@ -20,7 +20,6 @@ Workloads (rows, keys, values, functions):
 """
 from __future__ import annotations
 
-import math
 from dataclasses import dataclass
 from typing import List
 
