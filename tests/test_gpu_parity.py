@@ -292,3 +292,23 @@ def test_emit_into_caller_buffers(cuda):
         agg.close()
         for p in bufs:
             lib.vr_host_free(p)
+
+
+def test_autotuner_records_a_choice_that_meets_the_oracle(cuda):
+    """vr_tune_search times every candidate shape on one device batch and
+    records the fastest; vr_tune_lookup returns it, and a handle created
+    with it gives the oracle's groups."""
+    import ctypes as C
+
+    w = G.plain(rows=200_017)
+    db, keep = Cc.to_device(w.batch())
+    sp = w.spec()
+    batch = db.ctypes()
+    best, rps = N.TuneChoice(), C.c_double()
+    rc = N.lib().vr_tune_search(C.byref(sp.spec), C.byref(batch), 1, C.byref(best), C.byref(rps))
+    assert rc == N.VR_OK and rps.value > 0
+    got = N.TuneChoice()
+    assert N.lib().vr_tune_lookup(C.byref(sp.spec), w.rows, C.byref(got)) == 1  # 1: a choice is recorded
+    assert (got.tier, got.threads, got.tile_rows, got.smem_slots, got.blocks_per_sm) == \
+        (best.tier, best.threads, best.tile_rows, best.smem_slots, best.blocks_per_sm)
+    check(w, [w.batch()], tune=best)

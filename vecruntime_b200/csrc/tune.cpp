@@ -139,7 +139,7 @@ int vr_tune_search(const vr_agg_spec* spec, const vr_batch* batch, int32_t iters
     vr_plan_info info;
     if (vr_agg_plan(spec, &info, nullptr, 0) != VR_OK) return VR_ERR_UNSUPPORTED;
     std::vector<vr_tune_choice> cands;
-    auto add = [&](int tier, int wa, int threads, int tile, int smem) {
+    auto add = [&](int tier, int wa, int threads, int tile, int smem, int ctas) {
         vr_tune_choice c;
         std::memset(&c, 0, sizeof(c));
         c.tier = tier;
@@ -147,18 +147,23 @@ int vr_tune_search(const vr_agg_spec* spec, const vr_batch* batch, int32_t iters
         c.threads = threads;
         c.tile_rows = tile;
         c.smem_slots = smem;
+        c.blocks_per_sm = ctas;
         cands.push_back(c);
     };
+    // direct tier: threads x tile x CTAs per SM around the measured best
+    // (two CTAs of 160 threads with 640-row tiles on the decimal report)
     if (info.direct_ok) {
-        for (int t : {256, 128})
-            for (int tile : {2048, 1024}) add(0, 0, t, tile, 0);
+        const int shapes[][3] = {{160, 640, 2}, {128, 512, 2}, {96, 384, 3}, {64, 256, 4}, {256, 1024, 1}};
+        for (const auto& sh : shapes) add(0, 0, sh[0], sh[1], 0, sh[2]);
     }
+    // hash tiers: the default shape (whole table in shared memory when it
+    // fits, else a cache sized to the batch), hot-key caches from 256 to
+    // 1,024 slots with tiles from 1,024 down to 256 rows, and HBM only
     for (int wa : {0, 1}) {
-        for (int tile : {2048, 1024}) {
-            add(1, wa, 256, tile, 0);
-            add(1, wa, 256, tile, 512);
-            add(2, wa, 256, tile, 0);
-        }
+        add(1, wa, 0, 0, 0, 0);
+        for (int tile : {1024, 512, 256})
+            for (int slots : {256, 512, 1024}) add(1, wa, 256, tile, slots, 2);
+        add(2, wa, 256, 1024, 0, 2);
     }
     double best_v = -1;
     cudaEvent_t e0, e1;
