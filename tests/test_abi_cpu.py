@@ -129,3 +129,45 @@ def test_jit_specialises_the_aggregate_kernel_without_a_gpu(workload, tier):
         pytest.skip("libnvrtc is not loadable here: " + log.value.decode())
     assert rc == N.VR_OK, log.value.decode()
     assert nbytes.value > 10_000
+
+
+def test_tuner_table_records_keeps_the_fastest_and_round_trips(tmp_path):
+    """The autotuner's table (host only): a choice recorded for (spec, rows)
+    is found for rows of the same power of two and not for others; a slower
+    measurement does not replace a faster one; save and load carry every
+    field."""
+    from vecruntime_b200 import datagen as G
+
+    lib = N.lib()
+    sp = G.plain(rows=1000).spec()
+    rows = 3_000_001  # a power-of-two bucket no GPU test's batches fall in
+    t = N.TuneChoice()
+    t.tier, t.warp_agg, t.threads, t.blocks_per_sm, t.tile_rows, t.smem_slots = 1, 1, 256, 2, 512, 512
+    t.table_capacity = 1 << 20
+    assert lib.vr_tune_record(C.byref(sp.spec), rows, C.byref(t), C.c_double(2e9)) == N.VR_OK
+    slower = N.TuneChoice()
+    slower.tier, slower.threads, slower.tile_rows = 2, 128, 1024
+    assert lib.vr_tune_record(C.byref(sp.spec), rows, C.byref(slower), C.c_double(1e9)) == N.VR_OK
+
+    fields = ("tier", "warp_agg", "threads", "blocks_per_sm", "tile_rows", "smem_slots", "table_capacity")
+    got = N.TuneChoice()
+    assert lib.vr_tune_lookup(C.byref(sp.spec), rows + 100_000, C.byref(got)) == 1
+    assert [getattr(got, f) for f in fields] == [getattr(t, f) for f in fields]
+    assert lib.vr_tune_lookup(C.byref(sp.spec), 1000, C.byref(got)) == 0
+
+    path = tmp_path / "tune.txt"
+    assert lib.vr_tune_save(str(path).encode()) == N.VR_OK
+    text = path.read_text()
+    # a file with that entry's threads changed, loaded back: the lookup follows it
+    lines = [ln for ln in text.splitlines() if ln and not ln.startswith("#")]
+    assert lines
+    edited = []
+    for ln in lines:
+        f = ln.split()
+        if int(f[5]) == 256 and int(f[7]) == 512:  # threads, tile_rows of the recorded choice
+            f[5] = "192"
+        edited.append(" ".join(f))
+    path.write_text("\n".join(edited) + "\n")
+    assert lib.vr_tune_load(str(path).encode()) == N.VR_OK
+    assert lib.vr_tune_lookup(C.byref(sp.spec), rows, C.byref(got)) == 1
+    assert got.threads == 192 and got.tile_rows == 512 and got.smem_slots == 512
