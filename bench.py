@@ -10,7 +10,8 @@ larger than the 126 MB L2; a 1 GiB write on the stream precedes each step's
 start event, so L2 is cold and the device is busy while the host submits the
 step). `e2e` is the same work through the public C ABI
 with pinned host buffers: H2D of the step's inputs (chunked, copies
-overlapping kernels) + the emitted groups copied back.
+overlapping kernels) + the emitted groups copied back into pinned output
+buffers allocated once and reused every step.
 
 Other workloads (--workload plain|highcard|batched|serving) print the same
 line for their own shape. --impl reference times the CPU port of the
