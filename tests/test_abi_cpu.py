@@ -114,7 +114,7 @@ def test_create_without_gpu_fails_loudly():
         vr.GpuHashAggregate(cols, [0], [vr.CountAgg()])
 
 
-@pytest.mark.parametrize("workload,tier", [("decimal_report", 0), ("plain", 1)])
+@pytest.mark.parametrize("workload,tier", [("decimal_report", 0), ("plain", 1), ("high_cardinality", 1)])
 def test_jit_specialises_the_aggregate_kernel_without_a_gpu(workload, tier):
     """NVRTC compiles the per-spec aggregate kernel for sm_100a on the host;
     the same source the runtime launches, so a compile error shows here."""
@@ -171,3 +171,16 @@ def test_tuner_table_records_keeps_the_fastest_and_round_trips(tmp_path):
     assert lib.vr_tune_load(str(path).encode()) == N.VR_OK
     assert lib.vr_tune_lookup(C.byref(sp.spec), rows, C.byref(got)) == 1
     assert got.threads == 192 and got.tile_rows == 512 and got.smem_slots == 512
+
+
+def test_plan_shares_accumulators_between_functions():
+    """The decimal report's seven functions need six accumulators: avg(qty)
+    reuses sum(qty)'s sum, and every count of a non-nullable input is the
+    row count."""
+    from vecruntime_b200 import datagen as G
+
+    sp = G.decimal_report(rows=100).spec()
+    info = N.PlanInfo()
+    types = (N.ColumnType * 64)()
+    assert N.lib().vr_agg_plan(C.byref(sp.spec), C.byref(info), types, 64) == N.VR_OK
+    assert info.num_ops == 6 and info.direct_ok == 1
