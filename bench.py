@@ -1,29 +1,50 @@
 """Benchmark of the GPU grouped aggregate (one JSON line on stdout, rank 0).
 
-Default workload: the low-cardinality decimal report aggregate (60M rows,
-two dictionary keys -> 6 groups, four DECIMAL(12,2) columns; sum(qty),
-sum(price), sum(price*(1-disc)), sum(price*(1-disc)*(1+tax)) in exact
-decimal, avg(qty), avg(disc), count(*)) -- the TPC-H Q1 shape the reference
-quotes its headline numbers on. A step is one pass of the aggregate over the
-whole input: table clear + aggregate kernel, inputs resident in HBM (2.4 GB,
-larger than the 126 MB L2; a 1 GiB write on the stream precedes each step's
-start event, so L2 is cold and the device is busy while the host submits the
-step). `e2e` is the same work through the public C ABI
-with pinned host buffers: H2D of the step's inputs (chunked, copies
-overlapping kernels) + the emitted groups copied back into pinned output
-buffers allocated once and reused every step.
+The default run (`--workload all`) measures the metric's own comparison and
+every other workload in one line:
 
-Other workloads (--workload plain|highcard|batched|serving) print the same
-line for their own shape. --impl reference times the CPU port of the
-reference's aggregate (oracle/) on the host cores instead.
+* top level -- batched uneven instances: 512 independent aggregates (rows
+  log-uniform 2^10..2^22, cardinality log-uniform 1..2^20; int64 key, int64 +
+  float64 values; count/sum/min/max) in ONE persistent launch replayed from a
+  CUDA graph. `value` = rows/s of that launch with the inputs resident in HBM
+  (6.7 GB, larger than the 126 MB L2); `one_launch_per_instance` times the
+  same instances with one launch per instance, each with its own launch
+  configuration, and `speedup_vs_one_launch_per_instance` is their ratio.
+  `e2e` is the same step through the public API from pinned host memory:
+  every instance's inputs copied host->device, the persistent launch, and
+  every instance's groups emitted into pinned host buffers.
+* `workloads.{decimal,highcard,plain}` -- the low-cardinality decimal report
+  (60M rows, dictionary keys, exact decimal sums of fused products), the
+  high-cardinality composite key (100M rows, Zipf(1.1) int64 x int32[16],
+  1% null keys) and the plain aggregation (1,048,576 rows, 1,000 groups).
+  A step is one table clear + one aggregate launch over a device-resident
+  batch; a 1 GiB write on the stream precedes each step's start event, so
+  L2 is cold and the device is busy while the host submits the step. `e2e`
+  goes through the public C ABI with pinned host buffers (chunked H2D
+  overlapping the kernels, groups emitted into pinned buffers).
+* `serving` -- 16 live queries fed by a seeded Poisson trace of 2,000
+  requests/s for 5 minutes (one GPU): p50/p99 latency, queue wait, rows/s,
+  the most requests in flight at once.
 
-Multi-GPU (torchrun): every rank aggregates its own replica of the workload
-(weak scaling, no collective on the data path); time = max over ranks.
+Every record carries `roofline` (algorithmic bytes / kernel time against the
+measured HBM copy bandwidth), `cpu_baseline` (the CPU port of the reference's
+aggregate on the host cores, a bounded sample) and `parity`: after the timed
+steps, the groups of the full-size run are compared with the CPU port of the
+reference (groups as a sorted multiset; keys, counts, integer and decimal
+sums and min/max bit-exact; FP64 sums within 1e-12 relative of a compensated
+sum). --workload decimal|plain|highcard|batched|serving prints one of them as
+its own line; --impl reference times the CPU port on the host cores instead.
+
+Multi-GPU (torchrun): every rank aggregates its own replica (weak scaling, no
+collective on the data path); time = max over ranks; serving, parity and the
+CPU legs run at one GPU only.
 """
 from __future__ import annotations
 
 import argparse
+import concurrent.futures as cf
 import ctypes as C
+import hashlib
 import json
 import os
 import sys
@@ -36,32 +57,50 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "rows/s & HBM GB/s (% of peak), batched vs plain on 1 B200; serving p50/p99 ms"
+FLUSH_BYTES = 1 << 30  # written on the step's stream before each step's start event
+KERNEL_SOURCES = ("agg_main.cuh", "agg_device.cuh", "agg_types.h", "vr_internal.h", "agg_kernels.cu", "batched.cu")
+
+# DRAM bytes (read + write) per aggregate launch from `ncu --metrics
+# dram__bytes_read.sum,dram__bytes_write.sum` captures, each with the sha1
+# prefix of the kernel sources it was taken on (KERNEL_SOURCES): a figure
+# whose sources changed since is reported as null, not carried over. The
+# decimal report's traffic is its input plus a fixed flush, so a capture at
+# `rows` scales with rows; a hash table's traffic follows its group count, so
+# those captures hold only at their own row count.
+TRAFFIC = {
+    # name: (kernel sources sha1 prefix, rows captured, GB per launch, scales with rows)
+    "decimal": ("", 8_000_000, (320.097792e6 + 4.176128e6) / 1e9, True),
+    "plain": ("", 1 << 20, (25.473792e6 + 6.912e3) / 1e9, False),
+    "highcard": ("", 100_000_000, (7.72e9 + 2.57e9) / 1e9, False),
+}
 
 
 def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
 
-# DRAM bytes (read + write) of one aggregate launch, from ncu captures
-# (dram__bytes_read.sum + dram__bytes_write.sum). The decimal report's traffic
-# is its input plus a fixed flush, so an 8M-row capture scales with rows
-# (profiles/aggregate_decimal_report_8M.md). A hash table's traffic follows
-# its group count, not the rows, so those figures hold only at the row count
-# they were captured at (profiles/aggregate_plain_1M.md,
-# profiles/aggregate_high_cardinality_100M.md).
-TRAFFIC_PER_ROW = {"decimal": (320.097792e6 + 4.176128e6) / 8_000_000}
-TRAFFIC_AT_ROWS = {"plain": (1 << 20, 25.473792e6 + 6.912e3), "highcard": (100_000_000, 7.72e9 + 2.57e9)}
-FLUSH_BYTES = 1 << 30  # written on the step's stream before each step's start event
+def kernel_sha() -> str:
+    h = hashlib.sha1()
+    for f in KERNEL_SOURCES:
+        with open(os.path.join(ROOT, "vecruntime_b200", "csrc", f), "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()[:12]
 
 
-def launch_traffic(w):
+def launch_traffic(name, rows):
     """(GB per launch, how it was obtained) or (None, why not)."""
     src = "ncu dram__bytes_read.sum + dram__bytes_write.sum"
-    if w.name in TRAFFIC_PER_ROW:
-        return TRAFFIC_PER_ROW[w.name] * w.rows / 1e9, f"GB per launch ({src}, 8M-row capture scaled by rows)"
-    at = TRAFFIC_AT_ROWS.get(w.name)
-    if at is not None and at[0] == w.rows:
-        return at[1] / 1e9, f"GB per launch ({src}, capture of this workload at {w.rows} rows)"
+    t = TRAFFIC.get(name)
+    if t is None:
+        return None, "no ncu capture of this workload"
+    sha, at, gb, scales = t
+    now = kernel_sha()
+    if sha != now:
+        return None, f"no ncu capture of the current kernel sources ({now}); the last one was taken on {sha or 'older sources'}"
+    if scales:
+        return gb * rows / at, f"GB per launch ({src}, {at}-row capture on kernel sources {sha}, scaled by rows)"
+    if rows == at:
+        return gb, f"GB per launch ({src}, capture of this workload on kernel sources {sha})"
     return None, "no capture at this row count (table traffic follows the group count, not the rows)"
 
 
@@ -70,7 +109,8 @@ def measured_peaks():
     if os.path.exists(p):
         with open(p) as f:
             d = json.load(f)
-        return float(d.get("hbm_gbs", 6650.0)), "measured"
+        if "hbm_gbs" in d:
+            return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
 
 
@@ -184,30 +224,32 @@ def pin(a, lib, bufs):
     p = C.c_void_p()
     rc = lib.vr_host_alloc(max(a.nbytes, 16), C.byref(p))
     assert rc == 0, "pinned allocation"
-    dst = np.ctypeslib.as_array((C.c_uint8 * a.nbytes).from_address(p.value)).view(a.dtype).reshape(a.shape)
+    dst = np.ctypeslib.as_array((C.c_uint8 * max(a.nbytes, 1)).from_address(p.value))[:a.nbytes]
+    dst = dst.view(a.dtype).reshape(a.shape)
     dst[...] = a
     bufs.append(p)
     return dst
 
 
-def pinned_copy(w, lib):
+def pinned_copy(w, lib, bufs):
     """The workload's columns copied into pinned host memory (vr_host_alloc)."""
     from vecruntime_b200 import columns as Cc
 
-    bufs = []
-
-    def pin_one(a):
-        return pin(a, lib, bufs)
-
     cols = []
     for c in w.columns:
-        n = Cc.Col(c.lane, pin_one(c.data), pin_one(c.validity), c.precision, c.scale, c.dict_size, c.nullable)
+        n = Cc.Col(c.lane, pin(c.data, lib, bufs), pin(c.validity, lib, bufs), c.precision, c.scale, c.dict_size,
+                   c.nullable)
         if c.lane == 4:
             n._n = c._n
         cols.append(n)
-    return cols, bufs
+    return cols
 
 
+def host_threads():
+    return os.cpu_count() or 1
+
+
+# ------------------------------------------------------------------ CPU legs
 def cpu_baseline(w, sample_rows, threads):
     """One timed pass of the oracle over the first `sample_rows` rows:
     (rows/s, seconds)."""
@@ -239,38 +281,87 @@ def cpu_sample(w, threads, target_s):
     return done / secs, desc
 
 
-# ------------------------------------------------------------------ our arm
-def run_ours(args, rank, world, device):
+def cpu_batched(ws, threads, target_s):
+    """The oracle over whole instances of the batched workload, one instance
+    per host thread at a time (one Spark task each), until about `target_s`
+    seconds of wall time have passed or every instance ran once.
+    Returns (rows/s, description)."""
+    from oracle import pyoracle as O
+
+    def one(w):
+        o = O.Oracle(w.spec())
+        o.update(w.batch(), 4096)
+        o.close()
+        return w.rows
+
+    t0 = time.perf_counter()
+    rows, done = 0, 0
+    with cf.ThreadPoolExecutor(max_workers=threads) as ex:
+        futs = []
+        it = iter(ws)
+        for w in it:  # keep every thread busy; stop feeding once the time is up
+            futs.append(ex.submit(one, w))
+            if len(futs) >= threads:
+                rows += futs.pop(0).result()
+                done += 1
+                if time.perf_counter() - t0 > target_s:
+                    break
+        for f in futs:
+            rows += f.result()
+            done += 1
+    secs = time.perf_counter() - t0
+    desc = (f"{done} of {len(ws)} instances ({rows} rows), {threads} threads (one instance per thread, "
+            f"4096-row batches), {secs:.1f} s")
+    return rows / secs, desc
+
+
+def check_parity(spec, got_types, got_arrays, got_n, batch, threads):
+    """The full-size run's groups against the CPU port of the reference."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle import pyoracle as O
+    from parity import compare_arrays
+
+    t0 = time.perf_counter()
+    o = O.Oracle(spec)
+    o.update_threads(batch, threads)
+    want_n = o.num_groups()
+    want = o.emit(O.ORC_FP_COMPENSATED)
+    wt = o.output_types
+    o.close()
+    bad, ex = compare_arrays(spec, got_types, got_arrays, got_n, wt, want, want_n)
+    return {"groups": int(got_n), "oracle_groups": int(want_n), "mismatches": int(bad),
+            "examples": [str(e) for e in ex[:3]], "rows_checked": int(batch.num_rows),
+            "rule": "sorted multiset of groups; exact but FP64 sums (1e-12 relative of a compensated sum)",
+            "oracle_s": round(time.perf_counter() - t0, 1)}
+
+
+# ------------------------------------------------------------------ single workloads
+def run_single(args, name, rank, world, device, check):
     import torch
 
     import vecruntime_b200 as vr
+    from vecruntime_b200 import datagen as G
     from vecruntime_b200 import native as N
 
     torch.cuda.set_device(device)
     lib = N.lib()
-    w = make_workload(args.workload, args.rows)
+    w = make_workload(name, args.rows if args.workload == name else None)
     log(f"[rank {rank}] workload {w.name}: {w.rows} rows, est groups {w.est_groups}")
     db, tensors = device_batch(w, device)
     agg = vr.GpuHashAggregate(w.columns, w.keys, w.functions, est_groups=w.est_groups, max_batch_rows=w.rows,
                               device=device, flags=N.VR_SPEC_TRACE)
     stream = torch.cuda.ExternalStream(agg.stream(), device=torch.device("cuda", device))
-    from vecruntime_b200 import datagen as G
-
     in_bytes = G.input_bytes(w)
     # before each step's start event, a 1 GiB write on the same stream: it
     # evicts the inputs from L2 (126 MB) when they would fit there, and it
     # keeps the device busy while the host submits the step, so the events
     # time the step's device work rather than the host's submission latency
     flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device=device)
-    # warm-up
     for _ in range(args.warmup):
         agg.reset()
         agg.consume(db)
         agg.sync()
-    groups = agg.num_groups()
     st0 = agg.stats()
-    kms0 = st0.total_kernel_ms
-    launches0 = st0.kernel_launches
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     dist_barrier(world)
     torch.cuda.synchronize(device)
@@ -287,53 +378,48 @@ def run_ours(args, rank, world, device):
     dist_barrier(world)
     step_ms = [a.elapsed_time(b) for a, b in ev]
     st1 = agg.stats()
-    kernel_ms = (st1.total_kernel_ms - kms0) / args.steps
-    launches = st1.kernel_launches - launches0
+    kernel_ms = (st1.total_kernel_ms - st0.total_kernel_ms) / args.steps
+    launches = st1.kernel_launches - st0.kernel_launches
     ms_per_step, value = weak_scaling(sum(step_ms), args.steps, w.rows, world, device)
-
+    groups = agg.num_groups()
     out_types = agg.output_types
+    parity = None
+    if check:
+        got = agg.emit()
+        parity = check_parity(w.spec(), out_types, got, groups, w.batch(), host_threads())
+        del got
+    agg.close()
+    del tensors, flush
+
     out_bytes = groups * output_row_bytes(out_types)
     alg_bytes = in_bytes + out_bytes
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (kernel_ms * 1e-3) / 1e9
-    traffic, traffic_unit = launch_traffic(w)
-    agg.close()
-    del tensors, flush
-
-    # end to end through the public API: pinned host buffers, H2D + D2H in the step
-    e2e = None
-    if not args.no_e2e:
-        e2e = run_e2e(args, w, lib, device, out_types)
-        if e2e is not None:
-            e2e["value"] = dist_min(e2e["value"], world, device) * world
-
-    result = {
-        "metric": METRIC,
-        "value": value,
-        "unit": "rows/s",
-        "n_gpus": world,
-        "steps": args.steps,
-        "warmup": args.warmup,
-        "ms_per_step": ms_per_step,
-        "higher_is_better": True,
-        "scaling": "weak",
-        "vs_baseline": None,
+    traffic, traffic_unit = launch_traffic(w.name, w.rows)
+    rec = {
+        "value": value, "unit": "rows/s", "ms_per_step": ms_per_step, "steps": args.steps, "warmup": args.warmup,
         "dtype": workload_dtype(w),
-        "data": "synthetic (seeded; shapes of the workload, no benchmark data reproduced)",
         "config": {"workload": workload_label(w), "rows_per_gpu": w.rows, "groups": groups,
                    "batch": "one device-resident batch per step",
                    "l2": "L2 flushed before each step (%d MB written on the stream outside the timed events; "
-                         "inputs %.3f GB)" % (FLUSH_BYTES >> 20, in_bytes / 1e9),
-                   "parallelism": f"replicas x{world}"},
+                         "inputs %.3f GB)" % (FLUSH_BYTES >> 20, in_bytes / 1e9)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
                      "traffic": traffic, "traffic_unit": traffic_unit,
                      "algorithmic_bytes_per_launch": alg_bytes, "kernel_ms": kernel_ms},
-        "e2e": e2e,
         "gpu_launches": launches,
         "clocks": clocks.summary(),
+        "parity": parity,
     }
-    return result, w
+    if not args.no_e2e:
+        e2e = run_e2e(args, w, lib, device)
+        e2e["value"] = dist_min(e2e["value"], world, device) * world
+        rec["e2e"] = e2e
+    if check and not args.no_cpu_baseline:
+        rate, desc = cpu_sample(w, host_threads(), args.cpu_seconds)
+        rec["cpu_baseline"] = {"value": rate, "unit": "rows/s", "cores": host_threads(), "kind": "port",
+                               "sample": desc}
+    return rec
 
 
 def workload_dtype(w):
@@ -349,78 +435,55 @@ def workload_label(w):
             }.get(w.name, w.name)
 
 
-def run_e2e(args, w, lib, device, out_types):
+def run_e2e(args, w, lib, device):
     import torch
 
     import vecruntime_b200 as vr
     from vecruntime_b200 import columns as Cc
     from vecruntime_b200 import datagen as G
 
-    cols, bufs = pinned_copy(w, lib)
+    bufs = []
+    cols = pinned_copy(w, lib, bufs)
     chunk = min(w.rows, args.chunk_rows)
     chunk -= chunk % 128 if chunk > 128 else 0
     agg = vr.GpuHashAggregate(w.columns, w.keys, w.functions, est_groups=w.est_groups, max_batch_rows=chunk,
                               device=device)
     stream = torch.cuda.ExternalStream(agg.stream(), device=torch.device("cuda", device))
-
-    def batches():
-        out = []
-        for lo in range(0, w.rows, chunk):
-            hi = min(w.rows, lo + chunk)
-            out.append(Cc.HostBatch([G.slice_col(c, lo, hi) for c in cols], hi - lo))
-        return out
-
-    bl = batches()
-    groups = 0
+    bl = []
+    for lo in range(0, w.rows, chunk):
+        hi = min(w.rows, lo + chunk)
+        bl.append(Cc.HostBatch([G.slice_col(c, lo, hi) for c in cols], hi - lo))
     in_bytes = G.input_bytes(w)
     d2h = 0
     times = []
     # the groups come back into pinned buffers allocated once (the first
     # warm-up step sizes them), as a caller with a pinned output pool would
-    out_pinned, out_bufs = None, []
-    for it in range(args.warmup + args.steps):
+    out_pinned = None
+    for it in range(max(1, args.warmup) + args.steps):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
         agg.reset()
         for hb in bl:
             agg.consume(hb)
-        groups = agg.num_groups()
         out = agg.emit(out=out_pinned) if out_pinned is not None else agg.emit()
         b.record(stream)
         torch.cuda.synchronize(device)
-        if it >= args.warmup:
+        if it >= max(1, args.warmup):
             times.append(a.elapsed_time(b))
         d2h = sum(d.nbytes + v.nbytes for d, v in out)
         if out_pinned is None:
-            out_pinned = [(pin(d, lib, out_bufs), pin(v, lib, out_bufs)) for d, v in out]
+            out_pinned = [(pin(d, lib, bufs), pin(v, lib, bufs)) for d, v in out]
     agg.close()
-    for p in bufs + out_bufs:
+    for p in bufs:
         lib.vr_host_free(p)
     ms = float(np.mean(times))
     return {"value": w.rows / (ms * 1e-3), "unit": "rows/s", "h2d_bytes_per_step": in_bytes,
             "d2h_bytes_per_step": d2h, "ms_per_step": ms, "chunk_rows": chunk}
 
 
-# ------------------------------------------------------------------ batched (C4)
-def batched_choice():
-    """The one launch configuration every instance of a batched launch shares:
-    the hash tier's two-CTAs-per-SM shape (1024-row tiles, 256 consumer
-    threads, a 256-slot shared hot-key cache in front of each instance's HBM
-    table). Measured on this workload (persistent launch, CUDA graph):
-    1024-row tiles x 256 slots 27.3 ms, 512 x 512 27.4, 512 x 256 28.2,
-    256 x 256 29.1, 1024 x 128 29.1, 256 x 1024 29.6 (every change of
-    instance flushes the whole cache, so the larger caches that pay for one
-    long batch do not pay here)."""
-    from vecruntime_b200 import native as N
-
-    t = N.TuneChoice()
-    t.tier, t.threads, t.tile_rows, t.smem_slots = 1, 256, 1024, 256
-    return t
-
-
-def run_batched(args, device):
-    """512 uneven instances (rows log-uniform 2^10..2^22, cardinality
-    log-uniform 1..2^20): one persistent launch replayed from a CUDA graph,
+# ------------------------------------------------------------------ batched
+def run_batched(args, rank, world, device, check):
+    """512 uneven instances: one persistent launch replayed from a CUDA graph
     against one launch per instance. A step resets every table and
     aggregates every instance's device-resident batch."""
     import torch
@@ -431,63 +494,177 @@ def run_batched(args, device):
     from vecruntime_b200 import native as N
 
     torch.cuda.set_device(device)
+    lib = N.lib()
     ws = G.batched_instances(n=args.instances)
-    log(f"[batched] {len(ws)} instances, {sum(w.rows for w in ws)} rows")
+    rows = sum(w.rows for w in ws)
+    in_bytes = sum(G.input_bytes(w) for w in ws)
+    log(f"[rank {rank}] batched: {len(ws)} instances, {rows} rows, {sum(w.est_groups for w in ws)} est groups")
     aggs, dbs, keep = [], [], []
     for w in ws:
+        # each instance's own launch configuration (the autotuner's choice for
+        # its rows and estimated groups); the persistent launch picks one block
+        # shape for all and keeps each instance's shared-memory strategy
         aggs.append(vr.GpuHashAggregate(w.columns, w.keys, w.functions, est_groups=w.est_groups,
-                                        max_batch_rows=w.rows, device=device, tune=batched_choice()))
+                                        max_batch_rows=w.rows, device=device))
         db, t = Cc.to_device(w.batch(), device)
         dbs.append(db)
         keep.append(t)
     stream = torch.cuda.Stream(device=device)
-    rows = sum(w.rows for w in ws)
-    in_bytes = sum(G.input_bytes(w) for w in ws)
 
-    def timed(b):
-        for _ in range(args.warmup):
+    def timed(b, steps, warmup):
+        for _ in range(warmup):
             b.run(stream.cuda_stream)
-        ms = []
-        for _ in range(args.steps):
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        dist_barrier(world)
+        torch.cuda.synchronize(device)
+        for e0, e1 in ev:
             e0.record(stream)
             b.run(stream.cuda_stream)
             e1.record(stream)
-            e1.synchronize()
-            ms.append(e0.elapsed_time(e1))
-        return float(np.mean(ms))
+        torch.cuda.synchronize(device)
+        dist_barrier(world)
+        return sum(a.elapsed_time(b) for a, b in ev)
 
-    torch.cuda.synchronize(device)
     with ClockSampler(device) as clocks:
         persistent = vr.GpuBatchedAggregate(aggs, dbs, mode=N.VR_BATCHED_PERSISTENT, use_graph=True)
-        ms_p = timed(persistent)
-        persistent.close()
-        plain = vr.GpuBatchedAggregate(aggs, dbs, mode=N.VR_BATCHED_PLAIN)
-        ms_l = timed(plain)
-        plain.close()
-    launches = 3  # zero, aggregate, status gather
+        ms_p, value = weak_scaling(timed(persistent, args.steps, args.warmup), args.steps, rows, world, device)
+    info = persistent.info()
+    plain = vr.GpuBatchedAggregate(aggs, dbs, mode=N.VR_BATCHED_PLAIN)
+    ms_l, value_l = weak_scaling(timed(plain, args.steps, args.warmup), args.steps, rows, world, device)
+    plain.close()
+    # the groups of the persistent launch (the plain one ran last: run it once more)
+    persistent.run(stream.cuda_stream)
+    groups = [a.num_groups() for a in aggs]
+    out_types = aggs[0].output_types
+    parity = None
+    if check:
+        parity = check_batched(aggs, ws)
+    persistent.close()
     peak, peak_kind = measured_peaks()
-    for a in aggs:
-        a.close()
-    return {
-        "metric": METRIC, "value": rows / (ms_p * 1e-3), "unit": "rows/s", "n_gpus": 1, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_p, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "int64/f64", "data": "synthetic (seeded; shapes of the workload, no benchmark data reproduced)",
+    out_bytes = sum(groups) * output_row_bytes(out_types)
+    alg = in_bytes + out_bytes
+    rec = {
+        "value": value, "unit": "rows/s", "ms_per_step": ms_p, "steps": args.steps, "warmup": args.warmup,
+        "dtype": "int64/f64",
         "config": {"workload": f"batched uneven instances: {len(ws)} aggregates, {rows} rows, rows log-uniform "
                                "2^10..2^22, cardinality log-uniform 1..2^20, int64 key, int64 + float64 values, "
-                               "count/sum/min/max", "mode": "one persistent launch replayed from a CUDA graph",
+                               "count/sum/min/max", "rows_per_gpu": rows, "groups": int(sum(groups)),
+                   "mode": "one persistent launch replayed from a CUDA graph (table clears, aggregate, "
+                           "status gather)",
+                   "launch": info,
                    "l2": "inputs larger than L2 (%.2f GB)" % (in_bytes / 1e9)},
-        "roofline": {"bound": "hbm", "achieved": in_bytes / (ms_p * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
-                     "frac": in_bytes / (ms_p * 1e-3) / 1e9 / peak, "peak_kind": peak_kind, "traffic": None,
-                     "algorithmic_bytes_per_launch": in_bytes, "kernel_ms": ms_p},
-        "one_launch_per_instance": {"value": rows / (ms_l * 1e-3), "unit": "rows/s", "ms_per_step": ms_l},
+        "roofline": {"bound": "hbm", "achieved": alg / (ms_p * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": alg / (ms_p * 1e-3) / 1e9 / peak, "peak_kind": peak_kind, "traffic": None,
+                     "traffic_unit": "no ncu capture of the batched launch",
+                     "algorithmic_bytes_per_launch": alg,
+                     "kernel_ms": ms_p, "kernel_ms_is": "the whole graph (table clears + aggregate + status gather)"},
+        "one_launch_per_instance": {"value": value_l, "unit": "rows/s", "ms_per_step": ms_l,
+                                    "launches_per_step": "per instance: table clear, control clear, aggregate"},
         "speedup_vs_one_launch_per_instance": ms_l / ms_p,
-        "gpu_launches": launches * args.steps,
+        "gpu_launches": 3 * args.steps,
         "clocks": clocks.summary(),
+        "parity": parity,
     }
+    if not args.no_e2e:
+        e2e = run_batched_e2e(args, ws, aggs, dbs, keep, lib, device, stream)
+        e2e["value"] = dist_min(e2e["value"], world, device) * world
+        rec["e2e"] = e2e
+    if check and not args.no_cpu_baseline:
+        rate, desc = cpu_batched(ws, host_threads(), args.cpu_seconds)
+        rec["cpu_baseline"] = {"value": rate, "unit": "rows/s", "cores": host_threads(), "kind": "port",
+                               "sample": desc}
+    for a in aggs:
+        a.close()
+    return rec
 
 
-# ------------------------------------------------------------------ serving (C5)
+def check_batched(aggs, ws):
+    """Every instance's groups against the oracle (one instance per host thread)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle import pyoracle as O
+    from parity import compare_arrays
+
+    t0 = time.perf_counter()
+    got = []
+    for a in aggs:
+        n = a.num_groups()
+        got.append((n, a.emit()))
+
+    def one(i):
+        w = ws[i]
+        o = O.Oracle(w.spec())
+        o.update(w.batch(), 4096)
+        want_n = o.num_groups()
+        want = o.emit(O.ORC_FP_COMPENSATED)
+        wt = o.output_types
+        o.close()
+        n, arrays = got[i]
+        bad, ex = compare_arrays(w.spec(), aggs[i].output_types, arrays, n, wt, want, want_n)
+        return bad, ex, want_n
+
+    bad, groups, examples, wrong = 0, 0, [], 0
+    with cf.ThreadPoolExecutor(max_workers=host_threads()) as ex:
+        for i, (b, e, g) in enumerate(ex.map(one, range(len(ws)))):
+            bad += b
+            groups += g
+            if b:
+                wrong += 1
+                examples += [f"instance {i}: {x}" for x in e[:1]]
+    return {"groups": int(sum(n for n, _ in got)), "oracle_groups": int(groups), "mismatches": int(bad),
+            "instances_with_mismatches": wrong, "examples": examples[:3],
+            "rows_checked": int(sum(w.rows for w in ws)),
+            "rule": "per instance, sorted multiset of groups; exact but FP64 sums (1e-12 relative of a compensated sum)",
+            "oracle_s": round(time.perf_counter() - t0, 1)}
+
+
+def run_batched_e2e(args, ws, aggs, dbs, keep, lib, device, stream):
+    """The batched step through the public API from pinned host memory: every
+    instance's input columns copied into its device batch, the persistent
+    launch, every instance's groups emitted into pinned host buffers."""
+    import torch
+
+    import vecruntime_b200 as vr
+    from vecruntime_b200 import native as N
+
+    bufs = []
+    src = []  # (pinned host tensor, device tensor) per input buffer
+    for w, tensors in zip(ws, keep):
+        arrays = [c.data for c in w.columns] + [c.validity for c in w.columns if c.validity is not None]
+        for a, t in zip(arrays, tensors):
+            p = pin(np.frombuffer(np.ascontiguousarray(a).tobytes(), np.uint8), lib, bufs)
+            src.append((torch.from_numpy(p), t[:p.nbytes]))
+    h2d = sum(h.numel() for h, _ in src)
+    persistent = vr.GpuBatchedAggregate(aggs, dbs, mode=N.VR_BATCHED_PERSISTENT, use_graph=True)
+    outs = None
+    times = []
+    for it in range(max(1, args.warmup) + args.steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        with torch.cuda.stream(stream):
+            for h, d in src:
+                d.copy_(h, non_blocking=True)
+        persistent.run(stream.cuda_stream)
+        if outs is None:
+            res = [agg.emit() for agg in aggs]
+            outs = [[(pin(d, lib, bufs), pin(v, lib, bufs)) for d, v in r] for r in res]
+        else:
+            for agg, o in zip(aggs, outs):
+                agg.emit(out=o)
+        b.record(stream)
+        torch.cuda.synchronize(device)
+        if it >= max(1, args.warmup):
+            times.append(a.elapsed_time(b))
+    d2h = sum(d.nbytes + v.nbytes for o in outs for d, v in o)
+    persistent.close()
+    for p in bufs:
+        lib.vr_host_free(p)
+    ms = float(np.mean(times))
+    rows = sum(w.rows for w in ws)
+    return {"value": rows / (ms * 1e-3), "unit": "rows/s", "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h), "ms_per_step": ms}
+
+
+# ------------------------------------------------------------------ serving
 def run_serving(args, device):
     """16 live queries (resident tables of 1e3..1e7 groups) fed by Poisson
     arrivals (args.rate requests/s in total) of batches with log-uniform
@@ -520,28 +697,30 @@ def run_serving(args, device):
                     Cc.longs(rng.integers(-10**6, 10**6, size=n, dtype=np.int64), nullable=False),
                     Cc.doubles(rng.standard_normal(n), nullable=False)]
             w = G.Workload(f"q{q}", cols, [0], fns, card, n)
-            pcols, pb = pinned_copy(w, lib)
-            bufs += pb
-            batches.append(Cc.HostBatch(pcols, n))
+            batches.append(Cc.HostBatch(pinned_copy(w, lib, bufs), n))
         qid = srv.open_query(cols, [0], fns, est_groups=card, max_batch_rows=max_rows)
         queries.append(qid)
         pool.append(batches)
     # the seeded trace: arrival times and (query, batch) picks
     n_req = int(args.rate * args.seconds)
     gaps = rng.exponential(1.0 / args.rate, size=n_req)
-    picks = [(int(rng.integers(0, 16)), int(rng.integers(0, 4))) for _ in range(n_req)]
+    picks = rng.integers(0, 16, size=n_req), rng.integers(0, 4, size=n_req)
     tickets, rows_done = [], 0
-    with ClockSampler(device) as clocks:
+    lat = []
+    with ClockSampler(device, period_s=0.05) as clocks:
         t0 = time.perf_counter()
         due = t0
-        for gap, (q, b) in zip(gaps, picks):
+        for gap, q, b in zip(gaps, picks[0], picks[1]):
             due += gap
             d = due - time.perf_counter()
             if d > 0:
                 time.sleep(d)
             tickets.append(srv.submit(queries[q], pool[q][b]))
             rows_done += pool[q][b].num_rows
-        lat = [srv.wait(t) for t in tickets]
+            if len(tickets) > 4096:  # collect finished tickets as the trace goes on
+                lat += [srv.wait(t) for t in tickets[:2048]]
+                del tickets[:2048]
+        lat += [srv.wait(t) for t in tickets]
         wall = time.perf_counter() - t0
     st = srv.stats()
     srv.close()
@@ -549,43 +728,55 @@ def run_serving(args, device):
         lib.vr_host_free(p)
     lat = np.array(lat)
     return {
-        "metric": METRIC, "value": rows_done / wall, "unit": "rows/s", "n_gpus": 1, "steps": n_req,
-        "warmup": 0, "ms_per_step": float(np.mean(lat)), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "int64/f64", "data": "synthetic (seeded trace; no benchmark data reproduced)",
+        "value": rows_done / wall, "unit": "rows/s", "steps": n_req, "ms_per_step": float(np.mean(lat)),
         "config": {"workload": f"serving loop: 16 live queries (1e3..1e7 groups), Poisson arrivals at "
                                f"{args.rate:g} requests/s for {args.seconds:g} s, batches of 4,096..1,048,576 "
-                               "rows from pinned host memory", "hbm_cap_gb": 120},
-        "serving": {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-                    "max_ms": float(lat.max()), "p99_wait_ms": st.p99_wait_ms, "p99_service_ms": st.p99_service_ms,
-                    "requests": n_req, "slots": args.slots, "admitted_immediately": st.admitted_immediately,
-                    "queued": st.queued, "rejected": st.rejected, "hbm_peak_gb": st.hbm_peak / 1e9,
-                    "offered_rows_per_s": rows_done / float(np.sum(gaps))},
-        "gpu_launches": int(st.completed),
+                               "rows from pinned host memory", "hbm_cap_gb": 120, "slots": args.slots},
+        "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+        "max_ms": float(lat.max()), "p99_wait_ms": st.p99_wait_ms, "p99_service_ms": st.p99_service_ms,
+        "requests": n_req, "admitted_immediately": st.admitted_immediately, "queued": st.queued,
+        "rejected": st.rejected, "max_in_flight": st.max_in_flight, "hbm_peak_gb": st.hbm_peak / 1e9,
+        "offered_rows_per_s": rows_done / float(np.sum(gaps)), "gpu_launches": int(st.completed),
         "clocks": clocks.summary(),
     }
 
 
 # ------------------------------------------------------------------ reference arm
 def run_reference(args):
-    """The CPU port of the reference's aggregate (oracle/) on the host cores:
-    bounded samples of the same workload, every host thread."""
-    threads = os.cpu_count() or 1
-    w = make_workload(args.workload, args.rows)
-    for _ in range(args.warmup):
-        cpu_baseline(w, min(w.rows, 1 << 20), threads)
-    # each step about args.cpu_seconds of work, the whole run about 3 minutes at most
-    per_step = min(args.cpu_seconds, 180.0 / max(1, args.steps))
-    rates = []
-    desc = ""
-    for _ in range(args.steps):
-        r, desc = cpu_sample(w, threads, per_step)
-        rates.append(r)
+    """The CPU port of the reference's aggregate (oracle/) on the host cores,
+    every host thread: bounded samples of the same workload as our arm."""
+    from vecruntime_b200 import datagen as G
+
+    threads = host_threads()
+    name = "batched" if args.workload in ("all", "batched") else args.workload
+    if name == "serving":
+        name = "batched"
+    per_step = min(args.cpu_seconds, 150.0 / max(1, args.steps + args.warmup))
+    rates, desc = [], ""
+    if name == "batched":
+        ws = G.batched_instances(n=args.instances)
+        label = (f"batched uneven instances: {len(ws)} aggregates, {sum(w.rows for w in ws)} rows, rows log-uniform "
+                 "2^10..2^22, cardinality log-uniform 1..2^20, int64 key, int64 + float64 values, count/sum/min/max")
+        for _ in range(args.warmup):
+            cpu_batched(ws[:threads], threads, 1.0)
+        for _ in range(args.steps):
+            r, desc = cpu_batched(ws, threads, per_step)
+            rates.append(r)
+        rows, dtype = sum(w.rows for w in ws), "int64/f64"
+    else:
+        w = make_workload(name, args.rows)
+        label, rows, dtype = workload_label(w), w.rows, workload_dtype(w)
+        for _ in range(args.warmup):
+            cpu_baseline(w, min(w.rows, 1 << 20), threads)
+        for _ in range(args.steps):
+            r, desc = cpu_sample(w, threads, per_step)
+            rates.append(r)
     value = float(np.median(rates))
     return {
         "metric": METRIC, "impl": "reference", "value": value, "unit": "rows/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": w.rows / value * 1e3,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": workload_dtype(w),
-        "data": "synthetic (seeded)", "config": {"workload": workload_label(w), "rows_per_gpu": w.rows},
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": rows / value * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
+        "data": "synthetic (seeded)", "config": {"workload": label, "rows_per_gpu": rows},
         "cpu_baseline": {"value": value, "unit": "rows/s", "cores": threads, "kind": "port",
                          "sample": "per step: " + desc},
         "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -624,22 +815,40 @@ def weak_scaling(total_ms, steps, rows_per_rank, world, device):
     return ms_per_step, rows_per_rank * world / (ms_per_step * 1e-3)
 
 
+def line(rec, world, args):
+    """The contract's JSON line around a record."""
+    out = {"metric": METRIC, "value": rec["value"], "unit": rec["unit"], "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": rec["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": rec.get("dtype", "int64/f64"),
+           "data": "synthetic (seeded; shapes of the workload, no benchmark data reproduced)"}
+    cfg = dict(rec["config"])
+    cfg["parallelism"] = f"replicas x{world}"
+    out["config"] = cfg
+    for k, v in rec.items():
+        if k not in out and k not in ("config",):
+            out[k] = v
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="decimal", choices=["decimal", "plain", "highcard", "batched", "serving"])
+    ap.add_argument("--workload", default="all",
+                    choices=["all", "decimal", "plain", "highcard", "batched", "serving"])
     ap.add_argument("--instances", type=int, default=512, help="batched: instances")
     ap.add_argument("--rate", type=float, default=2000.0, help="serving: requests/s")
-    ap.add_argument("--seconds", type=float, default=10.0, help="serving: trace length")
+    ap.add_argument("--seconds", type=float, default=300.0, help="serving: trace length")
     ap.add_argument("--slots", type=int, default=32, help="serving: requests in flight on the device")
     ap.add_argument("--rows", type=int, default=None)
     ap.add_argument("--chunk-rows", type=int, default=8 << 20)
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline sample length")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-parity", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -649,10 +858,10 @@ def main():
         if rank == 0:
             print(json.dumps(run_reference(args)), flush=True)
         return
-    if args.workload in ("batched", "serving"):
-        if rank == 0:  # one GPU: these shapes are about one device's scheduling
-            fn = run_batched if args.workload == "batched" else run_serving
-            print(json.dumps(fn(args, local)), flush=True)
+    if args.workload == "serving":
+        if rank == 0:  # one GPU: serving is about one device's scheduling
+            rec = run_serving(args, local)
+            print(json.dumps(line(rec, 1, args)), flush=True)
         return
 
     if world > 1:
@@ -662,19 +871,30 @@ def main():
         import torch.distributed as dist
 
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    result, w = run_ours(args, rank, world, local)
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        threads = os.cpu_count() or 1
-        rate, desc = cpu_sample(w, threads, args.cpu_seconds)
-        result["cpu_baseline"] = {"value": rate, "unit": "rows/s", "cores": threads, "kind": "port", "sample": desc}
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    check = rank == 0 and world == 1 and not args.no_parity
+    if args.workload == "all":
+        serving = None
+        if world == 1 and not args.no_serving:
+            # first, in a fresh process: nothing else has touched host or device memory yet
+            serving = run_serving(args, local)
+        rec = run_batched(args, rank, world, local, check)
+        rec["workloads"] = {}
+        for name in ("decimal", "highcard", "plain"):
+            rec["workloads"][name] = run_single(args, name, rank, world, local, check)
+        if serving is not None:
+            rec["serving"] = serving
+    elif args.workload == "batched":
+        rec = run_batched(args, rank, world, local, check)
+    else:
+        rec = run_single(args, args.workload, rank, world, local, check)
     if world > 1:
         import torch.distributed as dist
 
         dist.barrier()
         dist.destroy_process_group()
     if rank == 0:
-        print(json.dumps(result), flush=True)
+        print(json.dumps(line(rec, world, args)), flush=True)
 
 
 if __name__ == "__main__":

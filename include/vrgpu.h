@@ -278,15 +278,27 @@ int vr_hash_rows(int32_t num_keys, const vr_column_type* types, const vr_column*
  * columns, more is VR_ERR_INVALID. Enqueues on `stream` and returns without
  * waiting. Calls on one stream are ordered; calls that overlap in time on
  * other streams or threads share the scratch and race. The first call on a
- * device looks the scratch up; make it before any stream capture. */
+ * device looks the scratch up and keeps its address for the life of the
+ * process: a device reset (cudaDeviceReset) is not supported afterwards.
+ * Do not capture this call into a CUDA graph: it copies the descriptors
+ * from the caller's host arrays with cudaMemcpyAsync, and a captured copy
+ * would read those arrays again at every replay, after they may be gone. */
 int vr_hash_rows_noalloc(int32_t num_keys, const vr_column_type* types, const vr_column* keys,
                          int64_t num_rows, uint32_t* out_device, int32_t finish, void* stream);
 
 /* ---- batched persistent aggregation ------------------------------------
  * Many independent instances (Spark tasks' batches) in one persistent
  * launch, optionally replayed from a CUDA graph. No reference analogue:
- * the reference runs one task per thread (VectorHashAggregateExec.scala:248-302). */
+ * the reference runs one task per thread (VectorHashAggregateExec.scala:248-302).
+ * The instances share one spec shape (one kernel) and one tier; the
+ * persistent launch runs them all with one block shape and tile size, and
+ * keeps each instance's own shared-memory strategy (its handle's tuner or
+ * default choice): a shared-memory table that holds every group, a hot-key
+ * cache in front of its HBM table, or its HBM table alone. VR_BATCHED_PLAIN
+ * runs one launch per instance with each handle's own configuration. */
 enum vr_batched_mode { VR_BATCHED_PERSISTENT = 0, VR_BATCHED_PLAIN = 1 };
+
+typedef struct vr_tune_choice vr_tune_choice;
 
 typedef struct vr_batched_plan {
     int32_t num_instances;
@@ -294,17 +306,37 @@ typedef struct vr_batched_plan {
     const vr_batch* batches;   /* one device-resident batch per instance     */
     int32_t mode;              /* enum vr_batched_mode                        */
     int32_t use_graph;         /* capture once, replay on later calls         */
+    const vr_tune_choice* shape; /* persistent launch: consumer threads, tile
+                                  rows, CTAs per SM and the hot-key cache slots
+                                  (each 0 = default); NULL = every default    */
 } vr_batched_plan;
+
+typedef struct vr_batched_info {
+    int32_t threads;           /* consumer threads per block                   */
+    int32_t tile_rows;
+    int32_t stages;
+    int32_t blocks;            /* per launch                                   */
+    int32_t smem_bytes;        /* dynamic shared memory per block              */
+    int32_t smem_slots_max;    /* slots of the shared-memory area              */
+    int32_t whole_tables;      /* instances with every group in shared memory  */
+    int32_t caches;            /* instances with a hot-key cache before HBM    */
+    int32_t hbm_only;          /* instances probing HBM directly               */
+    int32_t jit;               /* 1: a kernel compiled for this spec and shape */
+    int64_t total_tiles;
+    int64_t total_rows;
+    int64_t table_bytes;       /* HBM tables cleared by each run               */
+} vr_batched_info;
 
 typedef struct vr_batched vr_batched;
 int vr_batched_create(const vr_batched_plan* plan, vr_batched** out);
 /* Resets every instance's table, then aggregates every instance's batch. */
 int vr_batched_run(vr_batched* b, void* stream);
+int vr_batched_get_info(const vr_batched* b, vr_batched_info* info);
 void vr_batched_destroy(vr_batched* b);
 
 /* ---- autotuner (table size, block shape, tier) keyed on rows and
  *      estimated cardinality ------------------------------------------- */
-typedef struct vr_tune_choice {
+struct vr_tune_choice {
     int32_t tier;           /* 0 direct, 1 shared cache + HBM, 2 HBM only           */
     int32_t warp_agg;       /* __match_any_sync pre-aggregation                     */
     int32_t threads;        /* consumer threads per block (0 = default)             */
@@ -312,7 +344,7 @@ typedef struct vr_tune_choice {
     int32_t tile_rows;      /* rows per staged tile, multiple of 128 (0 = default)  */
     int32_t smem_slots;     /* shared cache slots, power of two (0 = default)       */
     int64_t table_capacity; /* HBM slots, power of two (0 = from est_groups)        */
-} vr_tune_choice;
+};
 /* vr_agg_create with a forced configuration (tests, the tuner's search). */
 int vr_agg_create_tuned(const vr_agg_spec* spec, const vr_tune_choice* choice, vr_agg** out);
 /* Runs every candidate configuration on one device-resident batch, times it
@@ -371,6 +403,9 @@ typedef struct vr_srv_stats {
     int64_t hbm_peak;
     double p99_wait_ms;        /* submit -> admitted to the device             */
     double p99_service_ms;     /* admitted -> result ready                     */
+    int64_t max_in_flight;     /* most requests admitted to the device and not
+                                  yet complete at one time (> 1: requests of
+                                  different queries overlapped on the device) */
 } vr_srv_stats;
 
 typedef struct vr_srv vr_srv;

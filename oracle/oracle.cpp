@@ -497,6 +497,9 @@ int orc_agg_create(const vr_agg_spec* spec, orc_agg** out) {
     a->keys.assign(spec->key_columns, spec->key_columns + spec->num_keys);
     a->fns.assign(spec->fns, spec->fns + spec->num_fns);
     a->spec = *spec;
+    a->spec.columns = a->cols.data();
+    a->spec.key_columns = a->keys.data();
+    a->spec.fns = a->fns.data();
     a->slots.assign(2048, -1);  // INITIAL_CAPACITY * 2 (GroupKeyTable.java:574)
     a->mask = 2047;
     a->kvals.resize(a->keys.size());
@@ -740,15 +743,17 @@ int orc_hash_rows(int32_t nk, const vr_column_type* types, const vr_column* keys
     return VR_OK;
 }
 
-int orc_agg_run_threads(const vr_agg_spec* spec, const vr_batch* b, int32_t threads, int64_t chunk, double* seconds,
-                        int64_t* groups) {
-    if (!spec || !b || threads < 1) return VR_ERR_INVALID;
+// Rows split into `threads` contiguous partitions (one Spark task each), each
+// aggregated in `chunk` batches into its own table; parts[0] ends up holding
+// every partition's groups (the reference merges task partials in the Final
+// aggregate). Returns the first failing status.
+static int run_partitions(const vr_agg_spec* spec, const vr_batch* b, int32_t threads, int64_t chunk,
+                          std::vector<orc_agg*>& parts) {
     const int64_t n = b->num_rows;
-    std::vector<orc_agg*> parts(threads, nullptr);
+    parts.assign(threads, nullptr);
     for (int t = 0; t < threads; ++t)
         if (orc_agg_create(spec, &parts[t]) != VR_OK) return VR_ERR_INVALID;
     std::atomic<int> status(VR_OK);
-    auto t0 = std::chrono::steady_clock::now();
     std::vector<std::thread> ws;
     for (int t = 0; t < threads; ++t) {
         ws.emplace_back([&, t] {
@@ -783,11 +788,29 @@ int orc_agg_run_threads(const vr_agg_spec* spec, const vr_batch* b, int32_t thre
     }
     for (auto& w : ws) w.join();
     for (int t = 1; t < threads; ++t) orc_agg_merge(parts[0], parts[t]);
+    return status.load();
+}
+
+int orc_agg_run_threads(const vr_agg_spec* spec, const vr_batch* b, int32_t threads, int64_t chunk, double* seconds,
+                        int64_t* groups) {
+    if (!spec || !b || threads < 1) return VR_ERR_INVALID;
+    std::vector<orc_agg*> parts;
+    auto t0 = std::chrono::steady_clock::now();
+    int rc = run_partitions(spec, b, threads, chunk, parts);
     auto t1 = std::chrono::steady_clock::now();
     if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
-    if (groups) *groups = parts[0]->size;
+    if (groups) *groups = parts[0] ? parts[0]->size : 0;
     for (auto* p : parts) orc_agg_destroy(p);
-    return status.load();
+    return rc;
+}
+
+int orc_agg_update_threads(orc_agg* dst, const vr_batch* b, int32_t threads, int64_t chunk) {
+    if (!dst || !b || threads < 1) return VR_ERR_INVALID;
+    std::vector<orc_agg*> parts;
+    int rc = run_partitions(&dst->spec, b, threads, chunk, parts);
+    if (rc == VR_OK && parts[0]) rc = orc_agg_merge(dst, parts[0]);
+    for (auto* p : parts) orc_agg_destroy(p);
+    return rc;
 }
 
 }  // extern "C"

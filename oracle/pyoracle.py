@@ -46,6 +46,7 @@ def lib():
         L.orc_agg_destroy.restype = None
         L.orc_last_error.restype = C.c_char_p
         L.orc_hash_rows.argtypes = [C.c_int32, C.POINTER(N.ColumnType), C.POINTER(N.Column), C.c_int64, P, C.c_int32]
+        L.orc_agg_update_threads.argtypes = [P, C.POINTER(N.Batch), C.c_int32, C.c_int64]
         L.orc_agg_run_threads.argtypes = [C.POINTER(N.AggSpec), C.POINTER(N.Batch), C.c_int32, C.c_int64,
                                           C.POINTER(C.c_double), C.POINTER(C.c_int64)]
         _lib = L
@@ -77,6 +78,14 @@ class Oracle:
     def update(self, batch, chunk_rows: int = 4096) -> None:
         cb = batch.ctypes()
         rc = lib().orc_agg_update(self.h, C.byref(cb), chunk_rows)
+        if rc:
+            raise OracleError(rc, lib().orc_last_error().decode())
+
+    def update_threads(self, batch, threads: int, chunk_rows: int = 4096) -> None:
+        """The batch split into `threads` contiguous partitions aggregated on
+        that many host threads, then merged here (full-size parity checks)."""
+        cb = batch.ctypes()
+        rc = lib().orc_agg_update_threads(self.h, C.byref(cb), threads, chunk_rows)
         if rc:
             raise OracleError(rc, lib().orc_last_error().decode())
 

@@ -77,19 +77,32 @@ def test_reset_is_ordered_before_later_work(cuda):
             a.close()
 
 
-@pytest.mark.parametrize("mode,use_graph", [(N.VR_BATCHED_PERSISTENT, False), (N.VR_BATCHED_PERSISTENT, True),
-                                            (N.VR_BATCHED_PLAIN, False)])
-def test_batched_instances_match_the_oracle(cuda, mode, use_graph):
-    ws = G.batched_instances(n=24, max_log_rows=14, max_log_card=12)
+def _instances(n, max_log_rows=14, max_log_card=12, tune=None):
+    ws = G.batched_instances(n=n, max_log_rows=max_log_rows, max_log_card=max_log_card)
     aggs, dbs, keep = [], [], []
     for w in ws:
         aggs.append(vr.GpuHashAggregate(w.columns, w.keys, w.functions, est_groups=w.est_groups,
-                                        max_batch_rows=w.rows, tune=shared_choice()))
+                                        max_batch_rows=w.rows, tune=tune))
         db, t = Cc.to_device(w.batch())
         dbs.append(db)
         keep.append(t)
+    return ws, aggs, dbs, keep
+
+
+@pytest.mark.parametrize("mode,use_graph", [(N.VR_BATCHED_PERSISTENT, False), (N.VR_BATCHED_PERSISTENT, True),
+                                            (N.VR_BATCHED_PLAIN, False)])
+@pytest.mark.parametrize("own_choice", [True, False])
+def test_batched_instances_match_the_oracle(cuda, mode, use_graph, own_choice):
+    """Instances with their own launch choices (whole shared-memory tables for
+    the small cardinalities, hot-key caches for the large ones) or one shared
+    choice, in one persistent launch or one launch each."""
+    ws, aggs, dbs, keep = _instances(24, tune=None if own_choice else shared_choice())
     b = vr.GpuBatchedAggregate(aggs, dbs, mode=mode, use_graph=use_graph)
     try:
+        if mode == N.VR_BATCHED_PERSISTENT and own_choice:
+            info = b.info()
+            assert info["whole_tables"] > 0 and info["caches"] > 0, info
+            assert info["whole_tables"] + info["caches"] + info["hbm_only"] == len(ws)
         for run in range(2):  # the second run replays (graph) and must reset the tables
             b.run()
             for w, a in zip(ws, aggs):
@@ -101,13 +114,35 @@ def test_batched_instances_match_the_oracle(cuda, mode, use_graph):
             a.close()
 
 
-def test_batched_refuses_mixed_launch_shapes(cuda):
+@pytest.mark.parametrize("threads,tile,ctas,cache", [(128, 256, 2, 512), (256, 1024, 2, 0), (512, 512, 1, 1024)])
+def test_batched_launch_shapes_match_the_oracle(cuda, threads, tile, ctas, cache):
+    """The persistent launch's block shape is the caller's to choose (or the
+    default); every shape must give the oracle's groups, growth included
+    (cardinalities up to 2^15 against tables sized for far fewer)."""
+    ws, aggs, dbs, keep = _instances(16, max_log_rows=16, max_log_card=15)
+    shape = N.TuneChoice()
+    shape.threads, shape.tile_rows, shape.blocks_per_sm, shape.smem_slots = threads, tile, ctas, cache
+    b = vr.GpuBatchedAggregate(aggs, dbs, mode=N.VR_BATCHED_PERSISTENT, use_graph=True, shape=shape)
+    try:
+        info = b.info()
+        assert info["threads"] == threads and info["tile_rows"] == tile
+        b.run()
+        for w, a in zip(ws, aggs):
+            n = a.num_groups()
+            compare(w.spec(), a.output_types, a.emit(), n, *oracle_of(w, [w.batch()]))
+    finally:
+        b.close()
+        for a in aggs:
+            a.close()
+
+
+def test_batched_refuses_different_specs(cuda):
+    """One persistent launch runs one kernel: instances whose specs differ
+    (here one more function) are refused."""
     ws = G.batched_instances(n=2, max_log_rows=12, max_log_card=4)
-    other = shared_choice()
-    other.tile_rows = 512
-    aggs = [vr.GpuHashAggregate(ws[0].columns, ws[0].keys, ws[0].functions, max_batch_rows=ws[0].rows,
-                                tune=shared_choice()),
-            vr.GpuHashAggregate(ws[1].columns, ws[1].keys, ws[1].functions, max_batch_rows=ws[1].rows, tune=other)]
+    aggs = [vr.GpuHashAggregate(ws[0].columns, ws[0].keys, ws[0].functions, max_batch_rows=ws[0].rows),
+            vr.GpuHashAggregate(ws[1].columns, ws[1].keys, ws[1].functions + [A.CountAgg(1)],
+                                max_batch_rows=ws[1].rows)]
     dbs, keep = [], []
     for w in ws:
         db, t = Cc.to_device(w.batch())
@@ -156,6 +191,9 @@ def test_serving_mix_equals_alone_and_the_oracle(cuda):
             alone.close()
         st = srv.stats()
         assert st.completed == len(tickets) and st.rejected == 0
+        # requests of different queries were on the device at the same time
+        # (admitted and not yet complete), not drained one at a time
+        assert st.max_in_flight > 1, st.max_in_flight
         # the latency splits into waiting for admission and running on the device
         assert 0 <= st.p99_wait_ms <= st.max_ms and 0 < st.p99_service_ms <= st.max_ms
     finally:

@@ -273,13 +273,15 @@ class GpuBatchedAggregate:
     runs one task per thread (VectorHashAggregateExec.scala:248-302)."""
 
     def __init__(self, instances: Sequence["GpuHashAggregate"], device_batches: Sequence, mode: int = 0,
-                 use_graph: bool = False):
+                 use_graph: bool = False, shape: Optional[N.TuneChoice] = None):
         self._lib = N.lib()
         self.instances = list(instances)
         self._batches = list(device_batches)
         self._hs = (C.c_void_p * len(self.instances))(*[a.h.value for a in self.instances])
         self._bs = (N.Batch * len(self._batches))(*[b.ctypes() for b in self._batches])
-        plan = N.BatchedPlan(len(self.instances), self._hs, self._bs, mode, 1 if use_graph else 0)
+        self._shape = shape
+        plan = N.BatchedPlan(len(self.instances), self._hs, self._bs, mode, 1 if use_graph else 0,
+                             C.pointer(shape) if shape is not None else None)
         h = C.c_void_p()
         rc = self._lib.vr_batched_create(C.byref(plan), C.byref(h))
         if rc:
@@ -293,6 +295,13 @@ class GpuBatchedAggregate:
         rc = self._lib.vr_batched_run(self.h, C.c_void_p(stream) if stream else None)
         if rc:
             raise N.VrError(rc, "vr_batched_run: " + (self._lib.vr_thread_last_error() or b"").decode())
+
+    def info(self) -> dict:
+        """The persistent launch's block shape and how many instances use a
+        whole shared-memory table, a hot-key cache or HBM alone."""
+        i = N.BatchedInfo()
+        N.check(self._lib.vr_batched_get_info(self.h, C.byref(i)), "vr_batched_get_info")
+        return {name: getattr(i, name) for name, _ in N.BatchedInfo._fields_}
 
     def close(self) -> None:
         if self.h:

@@ -63,14 +63,14 @@ DeviceInfo& device_info(int device) {
     return d;
 }
 
-static int64_t next_pow2(int64_t x) {
+int64_t next_pow2(int64_t x) {
     int64_t p = 1;
     while (p < x) p <<= 1;
     return p;
 }
 static size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
 
-static int32_t stage_bytes_for(const Program& P, int T) {
+int32_t stage_bytes_for(const Program& P, int T) {
     int32_t b = 0;
     for (int c = 0; c < P.num_cols; ++c) {
         int w = P.col_width[c];
@@ -81,7 +81,7 @@ static int32_t stage_bytes_for(const Program& P, int T) {
     return b;
 }
 
-static void fill_layout(const Program& P, int T, StageLayout& L) {
+void fill_layout(const Program& P, int T, StageLayout& L) {
     int32_t off = 0;
     for (int c = 0; c < kMaxCols; ++c) {
         L.data_off[c] = -1;
@@ -118,7 +118,7 @@ constexpr int kMaxCtasPerSm = 4;
 // How many CTAs of `threads` consumer threads (plus the producer warp), each
 // with `smem` dynamic shared bytes and `regs` registers per thread (0 =
 // unknown), fit on one SM together, at most `want`.
-static int ctas_per_sm(const DeviceInfo& di, int smem, int regs, int threads, int want) {
+int ctas_per_sm(const DeviceInfo& di, int smem, int regs, int threads, int want) {
     const int block = threads + 32;
     const int rb = (regs + 7) / 8 * 8;
     int k = 1;
@@ -647,6 +647,7 @@ void fill_desc(vr_agg* h, const vr_batch& b, BatchDesc& d, uint64_t* ctrl, const
     d.tier = h->cfg.tier;
     d.smem_slots = h->cfg.smem_slots;
     d.warp_agg = h->cfg.warp_agg;
+    d.s_probes = h->cfg.s_probes;
 }
 
 static bool tma_ok(const vr_agg* h, const BatchDesc& d) {
@@ -1162,7 +1163,14 @@ int vr_host_unregister(void* p) { return cudaHostUnregister(p) == cudaSuccess ? 
 
 int vr_hash_rows(int32_t num_keys, const vr_column_type* types, const vr_column* keys, int64_t num_rows,
                  uint32_t* out_device, int32_t finish, void* stream) {
-    if (num_keys < 0 || num_keys > 16 || (num_keys > 0 && (!types || !keys)) || !out_device) return VR_ERR_INVALID;
+    if (num_keys < 0 || (num_keys > 0 && (!types || !keys)) || !out_device) {
+        t_last_error = "vr_hash_rows: null descriptor or output pointer, or a negative key count";
+        return VR_ERR_INVALID;
+    }
+    if (num_keys > 16) {
+        t_last_error = "vr_hash_rows: " + std::to_string(num_keys) + " key columns, at most 16";
+        return VR_ERR_INVALID;
+    }
     cudaStream_t st = (cudaStream_t)stream;
     vr_column_type* td = nullptr;
     vr_column* kd = nullptr;

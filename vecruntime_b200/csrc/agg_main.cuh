@@ -647,7 +647,7 @@ VR_DEV void consume_tile(const Program& P, const BatchDesc& D, const LaunchCfg& 
                 r[j] = base + j * NT + ctid;
                 live[j] = r[j] < rows && (v.sel == nullptr || bit_at(v.sel, r[j]));
             }
-            hash_chunk<KW, R>(P, D, v, r, live, row0, tier, ss, cfg.s_probes, cfg.g_probes, wa, new_groups);
+            hash_chunk<KW, R>(P, D, v, r, live, row0, tier, ss, D.s_probes, cfg.g_probes, wa, new_groups);
         }
     }
 }
@@ -716,7 +716,11 @@ VR_DEV void aggregate_body(const BatchDesc* __restrict__ descs, const LaunchCfg&
                 consumer_bar(NT);
             }
             coop_copy(&D, &descs[inst], (int)sizeof(BatchDesc), ctid, NT);
-            zero_words(tier, cfg.tier_bytes / 8, ctid, NT);
+            // the next instance's part of the tier area (a batched launch
+            // mixes small whole tables and hot-key caches)
+            const int used = TIER == kTierDirect ? cfg.tier_bytes / 8
+                                                 : min(descs[inst].smem_slots, sslots) * VR_PSW(P);
+            zero_words(tier, used, ctid, NT);
             consumer_bar(NT);
             cur = inst;
         }

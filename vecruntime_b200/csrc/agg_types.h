@@ -21,7 +21,7 @@ struct LaunchCfg {
     int32_t num_desc;          // instances in this launch
     int64_t total_tiles;
     int32_t g_probes;          // HBM table probe limit before a row is deferred
-    int32_t s_probes;          // shared-memory cache probe limit
+    int32_t s_probes;          // unused: the probe limit is per instance (BatchDesc::s_probes)
     int32_t smem_bytes;        // dynamic shared memory of the launch
     int32_t tier_bytes;        // shared memory of the tier area
     int32_t rchunk;            // rows per consumer thread per chunk: 2, 4 or 8 (direct), 1 (hash)

@@ -11,8 +11,10 @@
 
 #include <algorithm>
 #include <cstring>
+#include <string>
 #include <vector>
 
+#include "jit.h"
 #include "runtime.h"
 
 namespace vr {
@@ -52,16 +54,23 @@ struct vr_batched {
     uint64_t* counter = nullptr;
     uint64_t* ctrl_all_dev = nullptr;
     uint64_t* ctrl_all_host = nullptr;
-    vr::LaunchCfg cfg{};
+    vr::LaunchCfg cfg{};  // the persistent launch: one block shape for every instance
+    vr::JitKernel* jit = nullptr;
     int kw = 1, tier = vr::kTierHash, blocks = 0;
     int64_t total_tiles = 0;
     int64_t total_rows = 0;
+    vr_batched_info info{};
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaStream_t graph_stream = nullptr;  // the stream the graph was captured for
 };
 
 using namespace vr;
+
+static cudaError_t persistent_launch(vr_batched* b, const LaunchCfg& L, cudaStream_t st) {
+    if (b->jit) return jit_launch(b->jit, b->descs_dev, L, b->blocks, b->counter, st);
+    return launch_aggregate(b->kw, b->tier, b->descs_dev, L, b->blocks, b->counter, st);
+}
 
 static int batched_enqueue(vr_batched* b, cudaStream_t st) {
     cudaError_t e;
@@ -73,8 +82,7 @@ static int batched_enqueue(vr_batched* b, cudaStream_t st) {
         LaunchCfg L = b->cfg;
         L.total_tiles = b->total_tiles;
         L.num_desc = n;
-        // every instance shares the program: the first instance's kernel serves all
-        if ((e = agg_launch(b->inst[0], b->descs_dev, L, b->blocks, b->counter, st)) != cudaSuccess) return VR_ERR_CUDA;
+        if ((e = persistent_launch(b, L, st)) != cudaSuccess) return VR_ERR_CUDA;
     } else {
         for (int i = 0; i < n; ++i) {
             vr_agg* h = b->inst[i];
@@ -97,20 +105,116 @@ static int batched_enqueue(vr_batched* b, cudaStream_t st) {
     return VR_OK;
 }
 
+// The persistent launch's block shape (hash tier): one for every instance,
+// since the stage layout and the kernel's thread count are per launch.
+// Measured defaults: two CTAs per SM of 256 consumer threads, 512-row tiles
+// and two stages, which leave a 1,024-slot shared-memory area per CTA for
+// 80-byte slots (a whole table for up to ~700 groups).
+static int batched_shape(vr_batched* b, const vr_tune_choice* shape) {
+    vr_agg* h0 = b->inst[0];
+    const Program& P = h0->plan.prog;
+    const DeviceInfo& di = device_info(b->device);
+    const int threads = shape && shape->threads ? shape->threads : 256;
+    const int want_ctas = shape && shape->blocks_per_sm ? shape->blocks_per_sm : 2;
+    const int T = shape && shape->tile_rows ? shape->tile_rows : 512;
+    if (threads % 32 || threads > kMaxConsumerThreadsJit || T % 128 || T <= 0) {
+        set_thread_error("batched shape: threads must be a multiple of 32 up to 512, tiles a multiple of 128");
+        return VR_ERR_INVALID;
+    }
+    const int budget = want_ctas <= 1 ? di.smem_optin : std::min(di.smem_optin, di.smem_per_sm / want_ctas - di.smem_reserved);
+    const int stages = 2;
+    const int sb = stage_bytes_for(P, T);
+    const int base = smem_map(stages, sb, 0).total;
+    if (base + 64 * 8 * P.sw > budget) {
+        set_thread_error("batched shape: tiles too long for the shared memory of one block");
+        return VR_ERR_UNSUPPORTED;
+    }
+    int64_t area = 1;
+    while (area * 2 * 8 * P.sw <= budget - base) area *= 2;  // power-of-two tables
+    LaunchCfg& L = b->cfg;
+    L = h0->launch;
+    L.tile_rows = T;
+    L.stages = stages;
+    L.consumer_threads = threads;
+    L.rchunk = 1;
+    fill_layout(P, T, L.lay);
+    L.tier_bytes = (int32_t)(area * 8 * P.sw);
+    L.smem_bytes = smem_map(stages, sb, L.tier_bytes).total;
+    b->info.smem_slots_max = (int32_t)area;
+    // the spec's own kernel for this shape; the prebuilt one (up to 256 threads) otherwise
+    int regs = aggregate_kernel_regs(b->kw, kTierHash);
+    if (jit_enabled() && !(h0->spec.flags & VR_SPEC_NO_JIT)) {
+        JitShape js;
+        js.kw = P.kw;
+        js.tier = kTierHash;
+        js.rchunk = 1;
+        js.threads = threads;
+        js.min_blocks = ctas_per_sm(di, L.smem_bytes, 0, threads, want_ctas);
+        std::string why;
+        b->jit = jit_get(P, js, b->device, &why);
+        if (b->jit) regs = jit_regs(b->jit);
+    }
+    if (!b->jit && threads > kMaxConsumerThreads) {
+        set_thread_error("batched shape: more than 256 threads needs a per-spec kernel, which did not compile");
+        return VR_ERR_UNSUPPORTED;
+    }
+    b->blocks = di.sms * ctas_per_sm(di, L.smem_bytes, regs, threads, want_ctas);
+    return VR_OK;
+}
+
+// One instance's shared-memory strategy inside the persistent launch: its
+// handle's own choice (the tuner's, else the default for its rows and
+// estimated groups), fitted to the launch's shared-memory area.
+//   whole table  -- every group in shared memory, probed until found: kept
+//                   when the estimated groups fill at most 70% of a table
+//                   that fits the area;
+//   hot-key cache -- the first keys a CTA meets, two probes, then HBM;
+//   HBM only     -- the handle chose no shared memory (tier 2).
+static void instance_strategy(vr_batched* b, vr_agg* h, BatchDesc& d, int cache_slots) {
+    const int64_t area = b->info.smem_slots_max;
+    d.warp_agg = h->cfg.warp_agg;
+    if (h->cfg.smem_slots <= 0) {
+        d.smem_slots = 0;
+        d.s_probes = 0;
+        b->info.hbm_only++;
+        return;
+    }
+    const int64_t est = h->spec.est_groups;
+    if (h->cfg.s_probes > 2 && est > 0) {
+        const int64_t need = next_pow2(std::max<int64_t>(64, (est * 10 + 6) / 7));
+        if (need <= area) {
+            d.smem_slots = (int32_t)need;
+            d.s_probes = 64;
+            b->info.whole_tables++;
+            return;
+        }
+    }
+    d.smem_slots = (int32_t)std::min<int64_t>(std::min<int64_t>(cache_slots, area), next_pow2(h->cfg.smem_slots));
+    d.s_probes = 2;
+    b->info.caches++;
+}
+
 extern "C" {
 
 int vr_batched_create(const vr_batched_plan* plan, vr_batched** out) {
-    if (!plan || !out || plan->num_instances <= 0 || !plan->instances || !plan->batches) return VR_ERR_INVALID;
+    if (!plan || !out || plan->num_instances <= 0 || !plan->instances || !plan->batches) {
+        set_thread_error("batched plan: null or empty");
+        return VR_ERR_INVALID;
+    }
     *out = nullptr;
     vr_batched* b = new vr_batched();
     b->mode = plan->mode;
     b->use_graph = plan->use_graph != 0;
     const int n = plan->num_instances;
     vr_agg* h0 = plan->instances[0];
+    if (!h0) {
+        delete b;
+        set_thread_error("batched plan: null instance");
+        return VR_ERR_INVALID;
+    }
     b->device = h0->device;
     cudaSetDevice(b->device);
-    // every instance must share the program shape (one kernel, one stage layout)
-    int max_tier_bytes = 0;
+    // every instance shares the program (one kernel) and the tier
     for (int i = 0; i < n; ++i) {
         vr_agg* h = plan->instances[i];
         const vr_batch& bt = plan->batches[i];
@@ -125,10 +229,15 @@ int vr_batched_create(const vr_batched_plan* plan, vr_batched** out) {
             return VR_ERR_INVALID;
         }
         if (h->device != b->device || std::memcmp(&h->plan.prog, &h0->plan.prog, sizeof(Program)) != 0 ||
-            h->cfg.tier != h0->cfg.tier || h->cfg.tile_rows != h0->cfg.tile_rows || h->cfg.stages != h0->cfg.stages ||
-            h->cfg.threads != h0->cfg.threads) {
+            h->cfg.tier != h0->cfg.tier) {
             delete b;
-            set_thread_error("batched instances must share device, spec shape and block shape");
+            set_thread_error("batched instances must share device, spec shape and tier");
+            return VR_ERR_UNSUPPORTED;
+        }
+        if (h0->cfg.tier == kTierDirect && (h->cfg.tile_rows != h0->cfg.tile_rows || h->cfg.stages != h0->cfg.stages ||
+                                            h->cfg.threads != h0->cfg.threads)) {
+            delete b;
+            set_thread_error("direct-tier batched instances must share their block shape");
             return VR_ERR_UNSUPPORTED;
         }
         if (vr_agg_sync(h) != VR_OK) {
@@ -136,21 +245,29 @@ int vr_batched_create(const vr_batched_plan* plan, vr_batched** out) {
             set_thread_error("instance handle failed");
             return VR_ERR_STATE;
         }
-        max_tier_bytes = std::max(max_tier_bytes, h->launch.tier_bytes);
         b->inst.push_back(h);
     }
     b->kw = h0->plan.prog.kw;
     b->tier = h0->cfg.tier;
-    b->cfg = h0->launch;
-    b->cfg.tier_bytes = max_tier_bytes;
-    b->cfg.smem_bytes = smem_map(b->cfg.stages, b->cfg.lay.stage_bytes, max_tier_bytes).total;
-    const DeviceInfo& di = device_info(b->device);
-    // the first instance's kernel serves all: its CTAs per SM, if the
-    // batch's (largest) shared-memory footprint still allows them
-    b->blocks = std::min(h0->blocks, di.sms * (di.fits(2, b->cfg.smem_bytes) ? 2 : 1));
+    if (b->tier == kTierDirect) {
+        b->cfg = h0->launch;
+        b->jit = h0->jit;
+        b->blocks = h0->blocks;
+        b->info.smem_slots_max = 0;
+    } else {
+        int rc = batched_shape(b, plan->shape);
+        if (rc != VR_OK) {
+            delete b;
+            return rc;
+        }
+    }
+    b->info.jit = b->jit ? 1 : 0;
+    const int cache_slots =
+        plan->shape && plan->shape->smem_slots ? (int)next_pow2(plan->shape->smem_slots) : 256;
     // descriptors: instance i's tiles follow instance i-1's
     std::vector<ZeroSpan> spans;
     int64_t tile = 0;
+    const int64_t T = b->mode == VR_BATCHED_PERSISTENT ? b->cfg.tile_rows : 0;
     for (int i = 0; i < n; ++i) {
         vr_agg* h = b->inst[i];
         const vr_batch& bt = plan->batches[i];
@@ -162,6 +279,7 @@ int vr_batched_create(const vr_batched_plan* plan, vr_batched** out) {
             if (cudaMalloc(&s.deferred, (size_t)s.deferred_cap * 8) != cudaSuccess ||
                 cudaMalloc(&s.deferred_tmp, (size_t)s.deferred_cap * 8) != cudaSuccess) {
                 vr_batched_destroy(b);
+                set_thread_error("deferred-row lists: device memory");
                 return VR_ERR_OOM;
             }
         }
@@ -174,6 +292,10 @@ int vr_batched_create(const vr_batched_plan* plan, vr_batched** out) {
         }
         d.selection = (const uint32_t*)bt.selection;
         fill_desc(h, bt, d, s.ctrl_dev, s, b->mode == VR_BATCHED_PERSISTENT ? tile : 0);
+        if (T > 0) {  // the persistent launch's tiles and shared-memory strategy
+            d.num_tiles = (bt.num_rows + T - 1) / T;
+            if (b->tier != kTierDirect) instance_strategy(b, h, d, cache_slots);
+        }
         bool tma = h->cfg.tma != 0;
         for (int c = 0; c < h->plan.prog.num_cols; ++c)
             tma = tma && ((uintptr_t)d.col_data[c] & 15) == 0 && ((uintptr_t)d.col_valid[c] & 15) == 0;
@@ -184,8 +306,16 @@ int vr_batched_create(const vr_batched_plan* plan, vr_batched** out) {
         b->total_rows += bt.num_rows;
         spans.push_back(ZeroSpan{h->table, h->table_slots * h->plan.prog.sw});
         spans.push_back(ZeroSpan{s.ctrl_dev, CTRL_WORDS});
+        b->info.table_bytes += h->table_slots * h->plan.prog.sw * 8;
     }
     b->total_tiles = tile;
+    b->info.threads = b->mode == VR_BATCHED_PERSISTENT ? b->cfg.consumer_threads : 0;
+    b->info.tile_rows = b->mode == VR_BATCHED_PERSISTENT ? b->cfg.tile_rows : 0;
+    b->info.stages = b->mode == VR_BATCHED_PERSISTENT ? b->cfg.stages : 0;
+    b->info.blocks = b->mode == VR_BATCHED_PERSISTENT ? b->blocks : 0;
+    b->info.smem_bytes = b->mode == VR_BATCHED_PERSISTENT ? b->cfg.smem_bytes : 0;
+    b->info.total_tiles = tile;
+    b->info.total_rows = b->total_rows;
     cudaError_t e;
     spans.push_back(ZeroSpan{nullptr, 0});
     b->num_spans = (int)spans.size() - 1;
@@ -195,14 +325,26 @@ int vr_batched_create(const vr_batched_plan* plan, vr_batched** out) {
         (e = cudaMalloc(&b->ctrl_all_dev, (size_t)n * CTRL_WORDS * 8)) != cudaSuccess ||
         (e = cudaMallocHost(&b->ctrl_all_host, (size_t)n * CTRL_WORDS * 8)) != cudaSuccess) {
         vr_batched_destroy(b);
+        set_thread_error("batched descriptors: device memory");
         return VR_ERR_OOM;
     }
     // the tile counter is zeroed with the tables
     b->num_spans += 1;
     spans[spans.size() - 1] = ZeroSpan{b->counter, 8};
-    cudaMemcpy(b->descs_dev, b->descs.data(), sizeof(BatchDesc) * n, cudaMemcpyHostToDevice);
-    cudaMemcpy(b->spans_dev, spans.data(), sizeof(ZeroSpan) * spans.size(), cudaMemcpyHostToDevice);
+    if ((e = cudaMemcpy(b->descs_dev, b->descs.data(), sizeof(BatchDesc) * n, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(b->spans_dev, spans.data(), sizeof(ZeroSpan) * spans.size(), cudaMemcpyHostToDevice)) !=
+            cudaSuccess) {
+        vr_batched_destroy(b);
+        set_thread_error(std::string("batched descriptors: ") + cudaGetErrorString(e));
+        return VR_ERR_CUDA;
+    }
     *out = b;
+    return VR_OK;
+}
+
+int vr_batched_get_info(const vr_batched* b, vr_batched_info* info) {
+    if (!b || !info) return VR_ERR_INVALID;
+    *info = b->info;
     return VR_OK;
 }
 
@@ -271,8 +413,8 @@ int vr_batched_run(vr_batched* b, void* stream) {
             cudaMemcpy(b->descs_dev + i, &d, sizeof(BatchDesc), cudaMemcpyHostToDevice);
             ZeroSpan zs{h->table, h->table_slots * h->plan.prog.sw};
             cudaMemcpy(b->spans_dev + 2 * i, &zs, sizeof(ZeroSpan), cudaMemcpyHostToDevice);
-            if (b->exec) {  // the graph captured the old pointers in kernel arguments only via descs: still valid
-            }
+            // a captured graph reads the table pointers from these device
+            // descriptors and spans, not from its kernel arguments: it stays valid
         }
     }
     return status;

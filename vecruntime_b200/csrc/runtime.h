@@ -134,6 +134,13 @@ int agg_reserve(vr_agg* h, int64_t rows);
 cudaError_t agg_launch(vr_agg* h, const BatchDesc* descs, const LaunchCfg& L, int blocks, uint64_t* tile_counter,
                        cudaStream_t st);
 int64_t tiles_for(const vr_agg* h, int64_t rows);
+// Bytes of one pipeline stage of T rows, and where each column lands in it.
+int32_t stage_bytes_for(const Program& P, int T);
+void fill_layout(const Program& P, int T, StageLayout& L);
+// CTAs of `threads` consumer threads (plus the producer warp), `smem` dynamic
+// shared bytes and `regs` registers per thread (0: unknown) that fit one SM, at most `want`.
+int ctas_per_sm(const DeviceInfo& di, int smem, int regs, int threads, int want);
+int64_t next_pow2(int64_t x);
 // Why a batch breaks the spec's nullability (a bitmap on a non-nullable column), or null.
 const char* batch_nullability_error(const vr_agg* h, const vr_batch& b);
 void set_thread_error(const std::string& msg);

@@ -136,6 +136,7 @@ void dispatch_loop(vr_srv* s) {
             r->state = 1;
             r->t_admit = Clock::now();
             s->in_flight++;
+            s->st.max_in_flight = std::max<int64_t>(s->st.max_in_flight, s->in_flight);
             s->in_flight_bytes += r->bytes;
             q.in_flight++;
             s->st.hbm_in_use = s->table_bytes + s->in_flight_bytes;

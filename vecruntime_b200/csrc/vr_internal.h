@@ -132,6 +132,9 @@ struct BatchDesc {
     int32_t smem_slots;      // hash tier: shared-memory cache slots (0 = HBM only)
     int32_t warp_agg;
     int32_t tma;             // bulk copies allowed for this batch
+    int32_t s_probes;        // hash tier: shared-memory probe limit (a table holding every
+                             // group probes until it finds the key; a hot-key cache gives up soon)
+    int32_t pad_;
 };
 
 // control block words

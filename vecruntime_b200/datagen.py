@@ -142,8 +142,14 @@ def batched_instances(n: int = 512, seed: int = SEEDS["batched"], max_log_rows: 
         vi = rng.integers(-1_000_000, 1_000_001, size=rows, dtype=np.int64)
         vf = rng.standard_normal(rows)
         cols = [Cc.longs(k, nullable=False), Cc.longs(vi, nullable=False), Cc.doubles(vf, nullable=False)]
-        out.append(Workload(f"inst{i}", cols, [0], batched_functions(), card, rows))
+        out.append(Workload(f"inst{i}", cols, [0], batched_functions(), expected_distinct(rows, card), rows))
     return out
+
+
+def expected_distinct(rows: int, card: int) -> int:
+    """Expected distinct keys among `rows` uniform draws from `card` values:
+    the cardinality estimate a planner that knows the batch size would pass."""
+    return max(1, int(np.ceil(card * -np.expm1(-rows / card))))
 
 
 def batched_functions():

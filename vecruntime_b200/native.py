@@ -124,7 +124,15 @@ class PlanInfo(C.Structure):
 
 class BatchedPlan(C.Structure):
     _fields_ = [("num_instances", C.c_int32), ("instances", C.POINTER(C.c_void_p)),
-                ("batches", C.POINTER(Batch)), ("mode", C.c_int32), ("use_graph", C.c_int32)]
+                ("batches", C.POINTER(Batch)), ("mode", C.c_int32), ("use_graph", C.c_int32),
+                ("shape", C.POINTER(TuneChoice))]
+
+
+class BatchedInfo(C.Structure):
+    _fields_ = [("threads", C.c_int32), ("tile_rows", C.c_int32), ("stages", C.c_int32), ("blocks", C.c_int32),
+                ("smem_bytes", C.c_int32), ("smem_slots_max", C.c_int32), ("whole_tables", C.c_int32),
+                ("caches", C.c_int32), ("hbm_only", C.c_int32), ("jit", C.c_int32), ("total_tiles", C.c_int64),
+                ("total_rows", C.c_int64), ("table_bytes", C.c_int64)]
 
 
 class SrvConfig(C.Structure):
@@ -137,7 +145,7 @@ class SrvStats(C.Structure):
                 ("queued", C.c_int64), ("rejected", C.c_int64), ("rows", C.c_int64),
                 ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("max_ms", C.c_double),
                 ("mean_ms", C.c_double), ("hbm_in_use", C.c_int64), ("hbm_peak", C.c_int64),
-                ("p99_wait_ms", C.c_double), ("p99_service_ms", C.c_double)]
+                ("p99_wait_ms", C.c_double), ("p99_service_ms", C.c_double), ("max_in_flight", C.c_int64)]
 
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib", "libvrgpu.so")
@@ -168,6 +176,7 @@ PROTOTYPES = [
                                        _P]),
     ("vr_batched_create", C.c_int, [C.POINTER(BatchedPlan), C.POINTER(_P)]),
     ("vr_batched_run", C.c_int, [_P, _P]),
+    ("vr_batched_get_info", C.c_int, [_P, C.POINTER(BatchedInfo)]),
     ("vr_batched_destroy", None, [_P]),
     ("vr_tune_lookup", C.c_int, [C.POINTER(AggSpec), C.c_int64, C.POINTER(TuneChoice)]),
     ("vr_tune_record", C.c_int, [C.POINTER(AggSpec), C.c_int64, C.POINTER(TuneChoice), C.c_double]),
