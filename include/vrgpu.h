@@ -45,7 +45,7 @@
 extern "C" {
 #endif
 
-#define VRGPU_ABI_VERSION 1
+#define VRGPU_ABI_VERSION 2
 
 /* ---- status codes ------------------------------------------------------ */
 enum vr_status {
@@ -73,8 +73,10 @@ enum vr_lane {
     VR_FLOAT64 = 3,    /* keys group by raw bits (GroupKeyTable.java:2350-2353)    */
     VR_BOOL = 4,       /* bit-packed                                               */
     VR_DECIMAL128 = 5, /* DECIMAL(p>18, s): two LE int64 limbs (Decimal128.java:21-61) */
-    VR_DICT32 = 6      /* UTF8 key as a dictionary id (int32); GroupKeyTable keeps
+    VR_DICT32 = 6,     /* dictionary-encoded UTF8: int32 ids into a dictionary of
+                          strings (vr_column.dictionary); GroupKeyTable keeps
                           strings as ids (GroupKeyTable.java:27-36)                */
+    VR_UTF8 = 7        /* plain UTF8: bytes + n + 1 int32 offsets (vr_hash_rows only) */
 };
 
 typedef struct vr_column_type {
@@ -168,9 +170,29 @@ typedef struct vr_agg_spec {
 /* ---- batches ----------------------------------------------------------- */
 enum vr_location { VR_HOST = 0, VR_DEVICE = 1 };
 
+/* The strings a VR_DICT32 column's ids point into (an Arrow dictionary:
+ * `size` entries, offsets[size + 1] into `data`, optional entry validity;
+ * a null entry makes its rows null, GroupKeyTable.java:1388-1389). The struct
+ * itself is in host memory; its buffers live where the batch lives.
+ * `hashes` (optional) are the entries' HashKernels.hashBytes values
+ * (NULL_MARK 0x7F4A7C15 for a null entry), e.g. from vr_hash_dictionary; a
+ * caller that reuses one dictionary across batches computes them once. */
+typedef struct vr_dictionary {
+    int32_t size;
+    int32_t reserved;
+    const int32_t* offsets;
+    const uint8_t* data;
+    const uint8_t* validity;   /* NULL = every entry valid                  */
+    const uint32_t* hashes;    /* NULL = computed where needed              */
+} vr_dictionary;
+
 typedef struct vr_column {
-    const void* data;
-    const uint8_t* validity; /* NULL = all valid */
+    const void* data;          /* values; VR_UTF8: the UTF-8 bytes          */
+    const uint8_t* validity;   /* NULL = all valid                          */
+    const int32_t* offsets;    /* VR_UTF8: n + 1 offsets into data          */
+    const vr_dictionary* dictionary; /* VR_DICT32: the batch's dictionary;
+                                  NULL = the ids are the spec's own (the
+                                  caller keeps one dictionary for every batch) */
 } vr_column;
 
 typedef struct vr_batch {
@@ -267,16 +289,30 @@ int vr_host_register(void* p, size_t bytes);
 int vr_host_unregister(void* p);
 
 /* ---- row hash parity (HashKernels.init/mixColumn/finish,
- *      kernels/.../HashKernels.java:42-236). Device pointers; out[n]. ------ */
+ *      kernels/.../HashKernels.java:42-236). Device pointers; out[n]. ------
+ * Bit for bit the reference's row hash for every lane: INT32, INT64/FLOAT64
+ * (folded), BOOL, DECIMAL128 (Decimal128.hash, folded), VR_UTF8
+ * (HashKernels.hashBytes of each row's bytes, mixUtf8 :199-213) and
+ * VR_DICT32 (hashBytes of each row's dictionary entry, mixDictionary
+ * :215-236: the column must carry its dictionary). A null row mixes
+ * NULL_MARK. Synchronous: returns once out_device is written. */
 int vr_hash_rows(int32_t num_keys, const vr_column_type* types, const vr_column* keys,
                  int64_t num_rows, uint32_t* out_device, int32_t finish, void* stream);
+/* HashKernels.hashBytes (HashKernels.java:183-197) of every entry of a
+ * device-resident dictionary (NULL_MARK for a null entry) into
+ * out_device[dict->size]; enqueued on `stream`, no allocation. */
+int vr_hash_dictionary(const vr_dictionary* dict, uint32_t* out_device, void* stream);
 /* vr_hash_rows without any device allocation, for callers that must not
  * allocate (a serving thread whose cudaMalloc/cudaFree would synchronise the
  * device under other queries, an executor at its memory cap). No counterpart
  * in the reference, whose hashing runs on the JVM heap. The key descriptors go
  * to a fixed 640-byte device scratch inside the library: at most 16 key
- * columns, more is VR_ERR_INVALID. Enqueues on `stream` and returns without
- * waiting. Calls on one stream are ordered; calls that overlap in time on
+ * columns, more is VR_ERR_INVALID. A VR_DICT32 key must bring its
+ * dictionary's entry hashes (dictionary->hashes, device memory, e.g. from
+ * vr_hash_dictionary into the caller's buffer): computing them here would
+ * need a buffer of the dictionary's size. An id outside the dictionary is not
+ * reported (the call does not wait): such a row mixes 0 in that column.
+ * Enqueues on `stream` and returns without waiting. Calls on one stream are ordered; calls that overlap in time on
  * other streams or threads share the scratch and race. The first call on a
  * device looks the scratch up and keeps its address for the life of the
  * process: a device reset (cudaDeviceReset) is not supported afterwards.

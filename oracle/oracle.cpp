@@ -46,6 +46,20 @@ uint32_t finish(uint32_t h) {
     return h;
 }
 uint32_t fold(uint64_t v) { return (uint32_t)(v ^ (v >> 32)); }
+// HashKernels.hashBytes (HashKernels.java:183-197): little-endian 4-byte
+// words, then the remaining bytes packed low-first, xor the length.
+uint32_t hash_bytes(const uint8_t* p, int32_t len) {
+    uint32_t h = 0x1B873593u;
+    int32_t i = 0;
+    for (; i + 4 <= len; i += 4) {
+        uint32_t w;
+        std::memcpy(&w, p + i, 4);
+        h = mix32(h, w);
+    }
+    uint32_t tail = 0;
+    for (int shift = 0; i < len; ++i, shift += 8) tail |= (uint32_t)p[i] << shift;
+    return mix32(h, tail ^ (uint32_t)len);
+}
 uint64_t dec_hash(uint64_t hi, uint64_t lo) {
     uint64_t h = lo * 0x9E3779B97F4A7C15ull;
     h ^= (h >> 32) ^ (hi * 0xC2B2AE3D27D4EB4Full);
@@ -735,9 +749,31 @@ const char* orc_last_error(void) { return g_err.c_str(); }
 
 int orc_hash_rows(int32_t nk, const vr_column_type* types, const vr_column* keys, int64_t n, uint32_t* out,
                   int32_t fin) {
+    for (int k = 0; k < nk; ++k) {
+        if (types[k].lane == VR_DICT32 && !keys[k].dictionary) return fail(nullptr, VR_ERR_INVALID, "dictionary key without its dictionary");
+        if (types[k].lane == VR_UTF8 && !keys[k].offsets) return fail(nullptr, VR_ERR_INVALID, "UTF8 key without offsets");
+    }
     for (int64_t i = 0; i < n; ++i) {
         uint32_t h = SEED;
-        for (int k = 0; k < nk; ++k) h = mix32(h, key_hash_value(types[k].lane, key_at(types[k], keys[k], i)));
+        for (int k = 0; k < nk; ++k) {
+            const vr_column& c = keys[k];
+            uint32_t v;
+            if (c.validity && !bit(c.validity, i)) {
+                v = NULL_MARK;
+            } else if (types[k].lane == VR_UTF8) {  // mixUtf8 (HashKernels.java:199-213)
+                const int32_t o = c.offsets[i];
+                v = hash_bytes((const uint8_t*)c.data + o, c.offsets[i + 1] - o);
+            } else if (types[k].lane == VR_DICT32) {  // mixDictionary (HashKernels.java:215-236)
+                const vr_dictionary& d = *c.dictionary;
+                const int32_t id = ((const int32_t*)c.data)[i];
+                if (id < 0 || id >= d.size) return fail(nullptr, VR_ERR_INVALID, "dictionary id outside its dictionary");
+                v = d.validity && !bit(d.validity, id) ? NULL_MARK
+                                                       : hash_bytes(d.data + d.offsets[id], d.offsets[id + 1] - d.offsets[id]);
+            } else {
+                v = key_hash_value(types[k].lane, key_at(types[k], c, i));
+            }
+            h = mix32(h, v);
+        }
         out[i] = fin ? finish(h) : h;
     }
     return VR_OK;

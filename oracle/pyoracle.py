@@ -119,13 +119,15 @@ class Oracle:
 
 
 def hash_rows(columns, n: int, finish: bool = True) -> np.ndarray:
+    """HashKernels' row hash of host columns (VR_DICT32 keys with their dictionary)."""
+    from vecruntime_b200.columns import HostBatch
+
     types = (N.ColumnType * max(1, len(columns)))(*[c.ctype() for c in columns])
-    cols = (N.Column * max(1, len(columns)))()
-    for i, c in enumerate(columns):
-        cols[i].data = c.data.ctypes.data
-        cols[i].validity = c.validity.ctypes.data if c.validity is not None else None
+    cb = HostBatch(list(columns), n).ctypes()  # keeps the dictionaries' structs alive
     out = np.zeros(max(n, 1), np.uint32)
-    lib().orc_hash_rows(len(columns), types, cols, n, out.ctypes.data, 1 if finish else 0)
+    rc = lib().orc_hash_rows(len(columns), types, cb.columns, n, out.ctypes.data, 1 if finish else 0)
+    if rc:
+        raise OracleError(rc, lib().orc_last_error().decode())
     return out[:n]
 
 

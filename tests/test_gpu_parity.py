@@ -148,9 +148,12 @@ def test_high_cardinality_small_warp_agg(cuda):
 def test_row_hash_matches_the_oracle(cuda, finish):
     """vr_hash_rows against the oracle's restatement of HashKernels
     (HashKernels.java:42-236): every lane, nulls mixing NULL_MARK, NaN and
-    signed zeros in doubles, both limbs of DECIMAL128."""
+    signed zeros in doubles, both limbs of DECIMAL128, plain UTF8 strings
+    (mixUtf8) and dictionary strings with a null entry (mixDictionary: the
+    entry's bytes are hashed, not its id)."""
     import ctypes as C
 
+    from keycols import device_key_columns, string_values
     from oracle.pyoracle import hash_rows
 
     torch = cuda
@@ -161,6 +164,9 @@ def test_row_hash_matches_the_oracle(cuda, finish):
     d[rng.random(n) < 0.05] = np.nan
     d[rng.random(n) < 0.05] = -0.0
     d[rng.random(n) < 0.05] = 0.0
+    entries = string_values(rng, 300, 0.0)
+    entries[7] = None  # a null entry: its rows hash as null
+    dic = Cc.dictionary(entries)
     cols = [Cc.ints(rng.integers(-2**31, 2**31, n), nulls(0.1), nullable=True),
             Cc.longs(rng.integers(-2**63, 2**63 - 1, n, dtype=np.int64), nulls(0.05), nullable=True),
             Cc.doubles(d, nulls(0.02), nullable=True),
@@ -168,26 +174,39 @@ def test_row_hash_matches_the_oracle(cuda, finish):
             Cc.decimals128([int(x) * (1 << 64) + int(y) for x, y in zip(rng.integers(-2**62, 2**62, n),
                                                                         rng.integers(0, 2**63, n))],
                            38, 0, nulls(0.1), nullable=True),
-            Cc.dict_ids(rng.integers(0, 1000, n), 1000, nulls(0.01), nullable=True)]
+            Cc.dict_strings(rng.integers(0, len(entries), n), dic, nulls(0.01), nullable=True),
+            Cc.strings(string_values(rng, n, 0.05), nullable=True)]
     want = hash_rows(cols, n, finish=bool(finish))
-    keep = []
-    types = (N.ColumnType * len(cols))(*[c.ctype() for c in cols])
-    dev = (N.Column * len(cols))()
-    for i, c in enumerate(cols):
-        t = torch.from_numpy(np.ascontiguousarray(c.data).view(np.uint8).copy()).cuda()
-        dev[i].data = t.data_ptr()
-        keep.append(t)
-        if c.validity is not None:
-            v = torch.from_numpy(np.ascontiguousarray(c.validity).copy()).cuda()
-            dev[i].validity = v.data_ptr()
-            keep.append(v)
-    out = torch.empty(n, dtype=torch.int32, device="cuda")
-    stream = torch.cuda.current_stream().cuda_stream
-    rc = N.lib().vr_hash_rows(len(cols), types, dev, n, C.c_void_p(out.data_ptr()), finish, C.c_void_p(stream))
-    assert rc == N.VR_OK, N.lib().vr_thread_last_error()
-    torch.cuda.synchronize()
-    got = out.cpu().numpy().view(np.uint32)
-    assert np.array_equal(got, want), f"{int((got != want).sum())} of {n} hashes differ"
+    for with_hashes in (False, True):
+        types, dev, keep = device_key_columns(torch, cols, dict_hashes=with_hashes)
+        out = torch.empty(n, dtype=torch.int32, device="cuda")
+        stream = torch.cuda.current_stream().cuda_stream
+        rc = N.lib().vr_hash_rows(len(cols), types, dev, n, C.c_void_p(out.data_ptr()), finish, C.c_void_p(stream))
+        assert rc == N.VR_OK, N.lib().vr_thread_last_error()
+        torch.cuda.synchronize()
+        got = out.cpu().numpy().view(np.uint32)
+        assert np.array_equal(got, want), f"{int((got != want).sum())} of {n} hashes differ"
+
+
+def test_row_hash_refuses_ids_without_strings_and_ids_outside_the_dictionary(cuda):
+    """A VR_DICT32 key without its dictionary has no reference hash (the
+    reference always hashes the strings); an id past the dictionary's end is
+    reported, not read."""
+    import ctypes as C
+
+    from keycols import device_key_columns
+
+    torch = cuda
+    L = N.lib()
+    out = torch.empty(64, dtype=torch.int32, device="cuda")
+    bare = Cc.dict_ids(np.arange(64) % 5, 5)
+    types, dev, keep = device_key_columns(torch, [bare])
+    assert L.vr_hash_rows(1, types, dev, 64, C.c_void_p(out.data_ptr()), 1, None) == N.VR_ERR_INVALID
+    assert b"dictionary" in L.vr_thread_last_error()
+    past = Cc.dict_strings(np.arange(64) % 6, Cc.dictionary(["a", "b", "c", "d", "e"]))  # id 5 is past the end
+    types, dev, keep = device_key_columns(torch, [past])
+    assert L.vr_hash_rows(1, types, dev, 64, C.c_void_p(out.data_ptr()), 1, None) == N.VR_ERR_INVALID
+    assert b"outside" in L.vr_thread_last_error()
 
 
 def dictionary_workload(rows, seed, with_nulls=True):

@@ -60,6 +60,40 @@ def test_noalloc_hashes_match_the_allocating_entry_point_on_two_calls_in_a_row(c
         assert torch.equal(out, want), f"{lanes}: noalloc hashes differ"
 
 
+def test_noalloc_dictionary_keys_match_the_allocating_entry_point(cuda):
+    """Dictionary strings: the caller brings the entries' hashes (computed
+    once per dictionary with vr_hash_dictionary into its own buffer), since
+    this entry point has no room for them; both calls in a row agree with
+    vr_hash_rows, which computes them itself. Without the hashes the call is
+    refused before anything is enqueued."""
+    from keycols import device_key_columns, string_values
+    from vecruntime_b200 import columns as Cc
+
+    torch = cuda
+    L = N.lib()
+    rng = np.random.default_rng(7)
+    stream = torch.cuda.current_stream().cuda_stream
+    outs = []
+    for n in (20_011, 513):
+        entries = string_values(rng, 97, 0.02)
+        cols = [Cc.dict_strings(rng.integers(0, 97, n), Cc.dictionary(entries), rng.random(n) < 0.1, nullable=True),
+                Cc.longs(rng.integers(-(1 << 62), 1 << 62, n, dtype=np.int64))]
+        types, dev, keep = device_key_columns(torch, cols, dict_hashes=True)
+        out = torch.empty(n, dtype=torch.int32, device="cuda")
+        rc = L.vr_hash_rows_noalloc(2, types, dev, n, C.c_void_p(out.data_ptr()), 1, C.c_void_p(stream))
+        assert rc == N.VR_OK, L.vr_thread_last_error()
+        outs.append((n, cols, types, dev, keep, out))
+    for n, cols, types, dev, keep, out in outs:
+        plain_types, plain_dev, plain_keep = device_key_columns(torch, cols, dict_hashes=False)
+        want = torch.empty(n, dtype=torch.int32, device="cuda")
+        rc = L.vr_hash_rows(2, plain_types, plain_dev, n, C.c_void_p(want.data_ptr()), 1, C.c_void_p(stream))
+        assert rc == N.VR_OK, L.vr_thread_last_error()
+        torch.cuda.synchronize()
+        assert torch.equal(out, want), "noalloc dictionary hashes differ"
+        rc = L.vr_hash_rows_noalloc(2, plain_types, plain_dev, n, C.c_void_p(out.data_ptr()), 1, C.c_void_p(stream))
+        assert rc == N.VR_ERR_INVALID and b"hashes" in L.vr_thread_last_error()
+
+
 def test_noalloc_refuses_more_keys_than_its_scratch_holds(cuda):
     torch = cuda
     L = N.lib()

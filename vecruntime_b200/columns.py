@@ -13,10 +13,12 @@ from typing import List, Optional, Sequence
 
 import numpy as np
 
+import ctypes as C
+
 from . import native as N
 
 LANE_NAMES = {N.VR_INT32: "INT32", N.VR_INT64: "INT64", N.VR_FLOAT64: "FLOAT64", N.VR_BOOL: "BOOL",
-              N.VR_DECIMAL128: "DECIMAL128", N.VR_DICT32: "DICT32"}
+              N.VR_DECIMAL128: "DECIMAL128", N.VR_DICT32: "DICT32", N.VR_UTF8: "UTF8"}
 
 
 def pack_bits(mask) -> np.ndarray:
@@ -51,9 +53,45 @@ def dec128_to_ints(limbs: np.ndarray) -> List[int]:
     return out
 
 
+def _utf8_buffers(values):
+    """bytes/str values (None for a null) -> (int32 offsets, uint8 data, null mask)."""
+    raw = [b"" if v is None else (v.encode() if isinstance(v, str) else bytes(v)) for v in values]
+    offsets = np.zeros(len(raw) + 1, np.int32)
+    offsets[1:] = np.cumsum([len(b) for b in raw])
+    data = np.frombuffer(b"".join(raw) + b"\0" * 16, np.uint8).copy()  # padded: never empty
+    return offsets, data, np.array([v is None for v in values], bool)
+
+
+@dataclass
+class Dictionary:
+    """An Arrow string dictionary (the values a VR_DICT32 column's ids point
+    into): int32 offsets, UTF-8 bytes, optional entry validity. A null entry
+    makes the rows that point at it null (GroupKeyTable.java:1388-1389)."""
+    offsets: np.ndarray
+    data: np.ndarray
+    validity: Optional[np.ndarray] = None
+    hashes: Optional[np.ndarray] = None  # hashBytes per entry, optional
+
+    @property
+    def size(self) -> int:
+        return len(self.offsets) - 1
+
+    def ctypes(self) -> N.Dictionary:
+        return N.Dictionary(self.size, 0, self.offsets.ctypes.data, self.data.ctypes.data,
+                            self.validity.ctypes.data if self.validity is not None else None,
+                            self.hashes.ctypes.data if self.hashes is not None else None)
+
+
+def dictionary(entries) -> Dictionary:
+    """A dictionary from str/bytes entries (None = a null entry)."""
+    offsets, data, nulls = _utf8_buffers(entries)
+    return Dictionary(offsets, data, pack_bits(~nulls) if nulls.any() else None)
+
+
 @dataclass
 class Col:
-    """One input column: lane type, values and optional validity bitmap."""
+    """One input column: lane type, values and optional validity bitmap;
+    VR_UTF8 adds its offsets, VR_DICT32 may carry its dictionary."""
     lane: int
     data: np.ndarray
     validity: Optional[np.ndarray] = None
@@ -61,6 +99,8 @@ class Col:
     scale: int = 0
     dict_size: int = 0
     nullable: Optional[bool] = None
+    offsets: Optional[np.ndarray] = None
+    dictionary: Optional[Dictionary] = None
 
     @property
     def length(self) -> int:
@@ -113,6 +153,18 @@ def dict_ids(ids, dict_size, nulls=None, **kw) -> Col:
     return Col(N.VR_DICT32, v, _validity(nulls, len(v)), dict_size=dict_size, **kw)
 
 
+def strings(values, **kw) -> Col:
+    """A plain UTF8 column from str/bytes values (None = null)."""
+    offsets, data, nulls = _utf8_buffers(values)
+    return Col(N.VR_UTF8, data, pack_bits(~nulls) if nulls.any() else None, offsets=offsets, **kw)
+
+
+def dict_strings(ids, dict_: Dictionary, nulls=None, **kw) -> Col:
+    """A dictionary-encoded UTF8 column: ids into `dict_`, carried with it."""
+    v = np.ascontiguousarray(ids, dtype=np.int32)
+    return Col(N.VR_DICT32, v, _validity(nulls, len(v)), dictionary=dict_, **kw)
+
+
 def bools(values, nulls=None, **kw) -> Col:
     b = np.asarray(values, dtype=bool)
     c = Col(N.VR_BOOL, pack_bits(b), _validity(nulls, len(b)), dict_size=2, **kw)
@@ -130,10 +182,16 @@ class HostBatch:
 
     def ctypes(self) -> N.Batch:
         arr = (N.Column * max(1, len(self.columns)))()
+        keep = [arr]
         for i, c in enumerate(self.columns):
             arr[i].data = c.data.ctypes.data if c.data is not None and c.data.size else None
             arr[i].validity = c.validity.ctypes.data if c.validity is not None else None
-        self._keep = [arr]
+            arr[i].offsets = c.offsets.ctypes.data if c.offsets is not None else None
+            if c.dictionary is not None:
+                d = c.dictionary.ctypes()
+                keep.append(d)
+                arr[i].dictionary = C.pointer(d)
+        self._keep = keep
         sel = self.selection.ctypes.data if self.selection is not None else None
         return N.Batch(self.num_rows, arr, sel, N.VR_HOST, 0)
 

@@ -1161,33 +1161,122 @@ int vr_host_register(void* p, size_t bytes) {
 }
 int vr_host_unregister(void* p) { return cudaHostUnregister(p) == cudaSuccess ? VR_OK : VR_ERR_CUDA; }
 
+}  // extern "C"
+
+namespace vr {
+// The kernel's descriptor of key column c (hashes: the dictionary's entry
+// hashes for a VR_DICT32 key); an error message when the column cannot be
+// hashed as the reference hashes it.
+static const char* hash_key_of(const vr_column_type& t, const vr_column& k, const uint32_t* hashes, HashKey& out) {
+    std::memset(&out, 0, sizeof(out));
+    out.data = k.data;
+    out.validity = k.validity;
+    out.lane = t.lane;
+    switch (t.lane) {
+        case VR_INT32:
+        case VR_INT64:
+        case VR_FLOAT64:
+        case VR_BOOL:
+        case VR_DECIMAL128:
+            break;
+        case VR_UTF8:
+            if (!k.offsets) return "a VR_UTF8 key needs its offsets";
+            out.offsets = k.offsets;
+            break;
+        case VR_DICT32:
+            if (!k.dictionary) return "a VR_DICT32 key needs its dictionary (the reference hashes the strings)";
+            if (k.dictionary->size < 0) return "negative dictionary size";
+            out.dict_size = k.dictionary->size;
+            out.dict_hashes = hashes;
+            break;
+        default:
+            return "unknown key lane";
+    }
+    return nullptr;
+}
+}  // namespace vr
+
+extern "C" {
+
+int vr_hash_dictionary(const vr_dictionary* dict, uint32_t* out_device, void* stream) {
+    if (!dict || !out_device || dict->size < 0 || (dict->size > 0 && (!dict->offsets || !dict->data))) {
+        t_last_error = "vr_hash_dictionary: null dictionary, output or buffers, or a negative size";
+        return VR_ERR_INVALID;
+    }
+    cudaError_t e = launch_hash_dictionary(*dict, out_device, (cudaStream_t)stream);
+    if (e != cudaSuccess) {
+        t_last_error = cudaGetErrorString(e);
+        return VR_ERR_CUDA;
+    }
+    return VR_OK;
+}
+
 int vr_hash_rows(int32_t num_keys, const vr_column_type* types, const vr_column* keys, int64_t num_rows,
                  uint32_t* out_device, int32_t finish, void* stream) {
     if (num_keys < 0 || (num_keys > 0 && (!types || !keys)) || !out_device) {
         t_last_error = "vr_hash_rows: null descriptor or output pointer, or a negative key count";
         return VR_ERR_INVALID;
     }
-    if (num_keys > 16) {
-        t_last_error = "vr_hash_rows: " + std::to_string(num_keys) + " key columns, at most 16";
+    if (num_keys > kHashRowsScratchMaxKeys) {
+        t_last_error = "vr_hash_rows: " + std::to_string(num_keys) + " key columns, at most " +
+                       std::to_string(kHashRowsScratchMaxKeys);
         return VR_ERR_INVALID;
     }
     cudaStream_t st = (cudaStream_t)stream;
-    vr_column_type* td = nullptr;
-    vr_column* kd = nullptr;
-    cudaError_t e = cudaMalloc(&td, sizeof(vr_column_type) * 16);
-    if (e == cudaSuccess) e = cudaMalloc(&kd, sizeof(vr_column) * 16);
-    if (e == cudaSuccess && num_keys > 0)
-        e = cudaMemcpyAsync(td, types, sizeof(vr_column_type) * num_keys, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess && num_keys > 0) e = cudaMemcpyAsync(kd, keys, sizeof(vr_column) * num_keys, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = launch_hash_rows(num_keys, td, kd, num_rows, out_device, finish, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    cudaFree(td);
-    cudaFree(kd);
+    // device memory: the descriptors, an error word, and the entry hashes of
+    // dictionaries that come without them
+    size_t bytes = 256 + sizeof(HashKey) * kHashRowsScratchMaxKeys;
+    size_t dict_off[kHashRowsScratchMaxKeys] = {};
+    for (int c = 0; c < num_keys; ++c) {
+        if (types[c].lane == VR_DICT32 && keys[c].dictionary && !keys[c].dictionary->hashes) {
+            dict_off[c] = bytes;
+            bytes += ((size_t)std::max(0, keys[c].dictionary->size) * 4 + 255) & ~(size_t)255;
+        }
+    }
+    char* mem = nullptr;
+    cudaError_t e = cudaMalloc(&mem, bytes);
     if (e != cudaSuccess) {
         t_last_error = cudaGetErrorString(e);
-        return VR_ERR_CUDA;
+        return VR_ERR_OOM;
     }
-    return VR_OK;
+    uint32_t* bad = reinterpret_cast<uint32_t*>(mem);
+    HashKey* kd = reinterpret_cast<HashKey*>(mem + 256);
+    HashKey hk[kHashRowsScratchMaxKeys];
+    int rc = VR_OK;
+    for (int c = 0; c < num_keys && rc == VR_OK; ++c) {
+        const uint32_t* hashes = nullptr;
+        if (types[c].lane == VR_DICT32 && keys[c].dictionary) {
+            hashes = keys[c].dictionary->hashes;
+            if (!hashes) {
+                hashes = reinterpret_cast<const uint32_t*>(mem + dict_off[c]);
+                e = launch_hash_dictionary(*keys[c].dictionary, const_cast<uint32_t*>(hashes), st);
+                if (e != cudaSuccess) rc = VR_ERR_CUDA;
+            }
+        }
+        if (const char* why = hash_key_of(types[c], keys[c], hashes, hk[c])) {
+            t_last_error = std::string("vr_hash_rows: ") + why;
+            rc = VR_ERR_INVALID;
+        }
+    }
+    uint32_t bad_host = 0;
+    if (rc == VR_OK) {
+        if (e == cudaSuccess) e = cudaMemsetAsync(bad, 0, 4, st);
+        if (e == cudaSuccess && num_keys > 0) e = cudaMemcpyAsync(kd, hk, sizeof(HashKey) * num_keys, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = launch_hash_rows(num_keys, kd, num_rows, out_device, finish, bad, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&bad_host, bad, 4, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) {
+            t_last_error = cudaGetErrorString(e);
+            rc = VR_ERR_CUDA;
+        } else if (bad_host) {
+            t_last_error = "vr_hash_rows: a dictionary id lies outside its dictionary";
+            rc = VR_ERR_INVALID;
+        }
+    } else {
+        cudaStreamSynchronize(st);  // dictionary hashes already queued into `mem`
+    }
+    cudaFree(mem);
+    return rc;
 }
 
 // The same kernel as vr_hash_rows with its descriptor table in the library's
@@ -1207,6 +1296,22 @@ int vr_hash_rows_noalloc(int32_t num_keys, const vr_column_type* types, const vr
                        std::to_string(kHashRowsScratchMaxKeys);
         return VR_ERR_INVALID;
     }
+    HashKey hk[kHashRowsScratchMaxKeys];
+    for (int c = 0; c < num_keys; ++c) {
+        const uint32_t* hashes = nullptr;
+        if (types[c].lane == VR_DICT32 && keys[c].dictionary) {
+            hashes = keys[c].dictionary->hashes;
+            if (!hashes) {
+                t_last_error = "vr_hash_rows_noalloc: a VR_DICT32 key must bring its dictionary's entry hashes "
+                               "(vr_hash_dictionary)";
+                return VR_ERR_INVALID;
+            }
+        }
+        if (const char* why = hash_key_of(types[c], keys[c], hashes, hk[c])) {
+            t_last_error = std::string("vr_hash_rows_noalloc: ") + why;
+            return VR_ERR_INVALID;
+        }
+    }
     static std::mutex mu;
     static void* scratch_of[64] = {};
     int dev = 0;
@@ -1215,7 +1320,7 @@ int vr_hash_rows_noalloc(int32_t num_keys, const vr_column_type* types, const vr
         t_last_error = "vr_hash_rows_noalloc: device index above 63";
         return VR_ERR_UNSUPPORTED;
     }
-    char* scratch = nullptr;
+    HashKey* kd = nullptr;
     if (e == cudaSuccess) {
         std::lock_guard<std::mutex> lk(mu);
         if (!scratch_of[dev]) {
@@ -1223,15 +1328,11 @@ int vr_hash_rows_noalloc(int32_t num_keys, const vr_column_type* types, const vr
             e = hash_rows_scratch_address(&p);
             if (e == cudaSuccess) scratch_of[dev] = p;
         }
-        scratch = static_cast<char*>(scratch_of[dev]);
+        kd = static_cast<HashKey*>(scratch_of[dev]);
     }
     cudaStream_t st = (cudaStream_t)stream;
-    vr_column_type* td = reinterpret_cast<vr_column_type*>(scratch);
-    vr_column* kd = reinterpret_cast<vr_column*>(scratch + kHashRowsScratchKeysOffset);
-    if (e == cudaSuccess && num_keys > 0)
-        e = cudaMemcpyAsync(td, types, sizeof(vr_column_type) * num_keys, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess && num_keys > 0) e = cudaMemcpyAsync(kd, keys, sizeof(vr_column) * num_keys, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = launch_hash_rows(num_keys, td, kd, num_rows, out_device, finish, st);
+    if (e == cudaSuccess && num_keys > 0) e = cudaMemcpyAsync(kd, hk, sizeof(HashKey) * num_keys, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = launch_hash_rows(num_keys, kd, num_rows, out_device, finish, nullptr, st);
     if (e != cudaSuccess) {
         t_last_error = cudaGetErrorString(e);
         return VR_ERR_CUDA;

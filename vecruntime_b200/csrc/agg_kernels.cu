@@ -383,22 +383,57 @@ VR_DEV uint64_t jdec_hash(uint64_t hi, uint64_t lo) {
     return h;
 }
 
-__global__ void k_hash_rows(int nk, const vr_column_type* __restrict__ types, const vr_column* __restrict__ keys,
-                            int64_t n, uint32_t* __restrict__ out, int finish) {
+// HashKernels.hashBytes (HashKernels.java:183-197): 4-byte little-endian
+// words, then the tail bytes xor the length.
+VR_DEV uint32_t jhash_bytes(const uint8_t* p, int32_t len) {
+    uint32_t h = 0x1B873593u;
+    int32_t i = 0;
+    for (; i + 4 <= len; i += 4)
+        h = jmix32(h, (uint32_t)p[i] | ((uint32_t)p[i + 1] << 8) | ((uint32_t)p[i + 2] << 16) | ((uint32_t)p[i + 3] << 24));
+    uint32_t tail = 0;
+    for (int shift = 0; i < len; ++i, shift += 8) tail |= (uint32_t)p[i] << shift;
+    return jmix32(h, tail ^ (uint32_t)len);
+}
+
+constexpr uint32_t kNullMark = 0x7F4A7C15u;  // HashKernels.NULL_MARK
+
+__global__ void k_hash_dictionary(vr_dictionary d, uint32_t* __restrict__ out) {
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < d.size; k += (int64_t)gridDim.x * blockDim.x) {
+        const bool valid = d.validity == nullptr || ((d.validity[k >> 3] >> (k & 7)) & 1);
+        out[k] = valid ? jhash_bytes(d.data + d.offsets[k], d.offsets[k + 1] - d.offsets[k]) : kNullMark;
+    }
+}
+
+__global__ void k_hash_rows(int nk, const HashKey* __restrict__ keys, int64_t n, uint32_t* __restrict__ out,
+                            int finish, uint32_t* bad_id) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         uint32_t h = 0x2545F491u;
         for (int c = 0; c < nk; ++c) {
-            const vr_column& col = keys[c];
+            const HashKey& col = keys[c];
             bool valid = col.validity == nullptr || ((col.validity[i >> 3] >> (i & 7)) & 1);
             uint32_t v;
             if (!valid) {
-                v = 0x7F4A7C15u;
+                v = kNullMark;
             } else {
-                switch (types[c].lane) {
+                switch (col.lane) {
                     case VR_INT32:
-                    case VR_DICT32:
                         v = (uint32_t) reinterpret_cast<const int32_t*>(col.data)[i];
                         break;
+                    case VR_DICT32: {
+                        const int32_t id = reinterpret_cast<const int32_t*>(col.data)[i];
+                        if ((uint32_t)id < (uint32_t)col.dict_size) {
+                            v = col.dict_hashes[id];
+                        } else {
+                            v = 0;
+                            if (bad_id) *bad_id = 1;
+                        }
+                        break;
+                    }
+                    case VR_UTF8: {
+                        const int32_t o = col.offsets[i];
+                        v = jhash_bytes(reinterpret_cast<const uint8_t*>(col.data) + o, col.offsets[i + 1] - o);
+                        break;
+                    }
                     case VR_INT64:
                     case VR_FLOAT64:
                         v = jfold(reinterpret_cast<const uint64_t*>(col.data)[i]);
@@ -501,16 +536,22 @@ cudaError_t launch_emit(const Program* prog_dev, const EmitProgram* emit_dev, co
     return cudaGetLastError();
 }
 
-cudaError_t launch_hash_rows(int num_keys, const vr_column_type* types_dev, const vr_column* keys_dev, int64_t n,
-                             uint32_t* out, int finish, cudaStream_t stream) {
+cudaError_t launch_hash_rows(int num_keys, const HashKey* keys_dev, int64_t n, uint32_t* out, int finish,
+                             uint32_t* bad_id, cudaStream_t stream) {
     if (n <= 0) return cudaSuccess;
-    k_hash_rows<<<grid_for(n, 256), 256, 0, stream>>>(num_keys, types_dev, keys_dev, n, out, finish);
+    k_hash_rows<<<grid_for(n, 256), 256, 0, stream>>>(num_keys, keys_dev, n, out, finish, bad_id);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_hash_dictionary(const vr_dictionary& dict, uint32_t* out, cudaStream_t stream) {
+    if (dict.size <= 0) return cudaSuccess;
+    k_hash_dictionary<<<grid_for(dict.size, 256), 256, 0, stream>>>(dict, out);
     return cudaGetLastError();
 }
 
 // Fixed device scratch for vr_hash_rows_noalloc: the key-column descriptors
-// of one call (types first, then columns), so that entry point never has to
-// allocate the small table the kernel reads. One copy per device, shared by
+// of one call, so that entry point never has to allocate the small table the
+// kernel reads. One copy per device, shared by
 // every call on that device. Nothing here needs to start at zero: each call
 // writes the descriptors it uses before its kernel reads them.
 static __device__ __align__(256) unsigned char g_hash_rows_scratch[kHashRowsScratchBytes];

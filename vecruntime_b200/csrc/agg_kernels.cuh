@@ -43,18 +43,28 @@ cudaError_t launch_compact_kw(int kw, const uint64_t* table, int64_t slots, int 
 cudaError_t launch_emit(const Program* prog_dev, const EmitProgram* emit_dev, const uint64_t* table,
                         const int64_t* slot_of, int64_t from, int64_t to, const vr_out_column* outs_dev,
                         uint64_t* ctrl, cudaStream_t stream);
-// vr_hash_rows_noalloc's fixed scratch: at most this many key columns, their
-// vr_column_type entries at offset 0 and vr_column entries at
-// kHashRowsScratchKeysOffset.
+// One key column of the row hash, as the kernel reads it.
+struct HashKey {
+    const void* data;
+    const uint8_t* validity;      // nullptr: every row valid
+    const int32_t* offsets;       // VR_UTF8: n + 1 offsets into data
+    const uint32_t* dict_hashes;  // VR_DICT32: hashBytes of each dictionary entry
+    int32_t lane;
+    int32_t dict_size;            // VR_DICT32: entries; an id outside [0, dict_size) mixes 0
+};
+static_assert(sizeof(HashKey) == 40, "HashKey layout");
+// vr_hash_rows_noalloc's fixed scratch: at most this many key descriptors.
 constexpr int kHashRowsScratchMaxKeys = 16;
-constexpr size_t kHashRowsScratchKeysOffset = kHashRowsScratchMaxKeys * sizeof(vr_column_type);
-constexpr size_t kHashRowsScratchBytes = kHashRowsScratchKeysOffset + kHashRowsScratchMaxKeys * sizeof(vr_column);
+constexpr size_t kHashRowsScratchBytes = kHashRowsScratchMaxKeys * sizeof(HashKey);
 static_assert(kHashRowsScratchBytes == 640, "the header documents a 640-byte scratch");
 // The scratch's device address on the current device.
 cudaError_t hash_rows_scratch_address(void** out);
 
-// Reference row hash (HashKernels.java) over device key columns.
-cudaError_t launch_hash_rows(int num_keys, const vr_column_type* types_dev, const vr_column* keys_dev,
-                             int64_t n, uint32_t* out, int finish, cudaStream_t stream);
+// Reference row hash (HashKernels.java) over device key columns; `bad_id`
+// (optional) receives 1 when a dictionary id lies outside its dictionary.
+cudaError_t launch_hash_rows(int num_keys, const HashKey* keys_dev, int64_t n, uint32_t* out, int finish,
+                             uint32_t* bad_id, cudaStream_t stream);
+// HashKernels.hashBytes of every entry of a device dictionary (NULL_MARK for a null entry).
+cudaError_t launch_hash_dictionary(const vr_dictionary& dict, uint32_t* out, cudaStream_t stream);
 
 }  // namespace vr

@@ -23,7 +23,7 @@ VR_ERR_STATE = 8
 VR_ERR_ADMISSION = 9
 VR_ERR_DECIMAL_OVERFLOW = 10
 
-VR_INT32, VR_INT64, VR_FLOAT64, VR_BOOL, VR_DECIMAL128, VR_DICT32 = 1, 2, 3, 4, 5, 6
+VR_INT32, VR_INT64, VR_FLOAT64, VR_BOOL, VR_DECIMAL128, VR_DICT32, VR_UTF8 = 1, 2, 3, 4, 5, 6, 7
 
 VR_FN_COUNT_STAR = 1
 VR_FN_COUNT = 2
@@ -86,8 +86,14 @@ class AggSpec(C.Structure):
                 ("device", C.c_int32), ("flags", C.c_int32)]
 
 
+class Dictionary(C.Structure):
+    _fields_ = [("size", C.c_int32), ("reserved", C.c_int32), ("offsets", C.c_void_p), ("data", C.c_void_p),
+                ("validity", C.c_void_p), ("hashes", C.c_void_p)]
+
+
 class Column(C.Structure):
-    _fields_ = [("data", C.c_void_p), ("validity", C.c_void_p)]
+    _fields_ = [("data", C.c_void_p), ("validity", C.c_void_p), ("offsets", C.c_void_p),
+                ("dictionary", C.POINTER(Dictionary))]
 
 
 class Batch(C.Structure):
@@ -172,6 +178,7 @@ PROTOTYPES = [
     ("vr_host_register", C.c_int, [_P, C.c_size_t]),
     ("vr_host_unregister", C.c_int, [_P]),
     ("vr_hash_rows", C.c_int, [C.c_int32, C.POINTER(ColumnType), C.POINTER(Column), C.c_int64, _P, C.c_int32, _P]),
+    ("vr_hash_dictionary", C.c_int, [C.POINTER(Dictionary), _P, _P]),
     ("vr_hash_rows_noalloc", C.c_int, [C.c_int32, C.POINTER(ColumnType), C.POINTER(Column), C.c_int64, _P, C.c_int32,
                                        _P]),
     ("vr_batched_create", C.c_int, [C.POINTER(BatchedPlan), C.POINTER(_P)]),
