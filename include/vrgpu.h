@@ -112,7 +112,15 @@ enum vr_fn_kind {
 enum vr_fn_flags {
     VR_FN_CHECKED = 1,          /* ANSI bigint sum: overflow -> VR_ERR_OVERFLOW      */
     VR_FN_NULL_ON_OVERFLOW = 2, /* non-ANSI decimal: past precision -> null          */
-    VR_FN_FINAL = 4,            /* Final / Complete result in the sum slot           */
+    VR_FN_FINAL = 4,            /* Final / Complete: the function's result in its first
+                                   slot (Spark's evaluateExpression over the merged
+                                   buffer): a decimal sum checked against its precision;
+                                   avg(double) = sum / count, null for no rows
+                                   (Average, VectorAggregates.scala:1065-1090); a decimal
+                                   avg = sum / count at the result type with Spark's
+                                   half-up division (DecimalAvgResult,
+                                   VectorAggregates.scala:405-430). The count stays in
+                                   the second slot, as the reference emits it.        */
     VR_FN_STRICT = 8            /* accepted for parity with spark.vecruntime.exec.strictFloatingPoint;
                                    FP64 sums are compensated, not sequential          */
 };
@@ -140,6 +148,11 @@ typedef struct vr_agg_fn {
                                   or VR_ERR_DECIMAL_PRECISION with VR_FN_CHECKED,
                                   Spark's CheckOverflow on the multiply            */
     vr_term terms[3];
+    int32_t result_precision; /* VR_FN_FINAL decimal avg: the result type, Spark's
+                                 Decimal(p + 4, s + 4) of the input decimal(p, s),
+                                 bounded to 38; 0 = derived from the buffer type
+                                 (Decimal(p + 10, s), which must then be below 38) */
+    int32_t result_scale;
 } vr_agg_fn;
 
 enum vr_spec_flags {

@@ -427,6 +427,85 @@ void add_out(orc_agg* a, int lane, int precision, int scale) {
 
 // Output schema: keys, then each function's Spark buffer slots
 // (VectorAggFunction.bufferTypes, VectorAggregates.scala).
+// A decimal average's result type: given, or Spark's Decimal(p + 4, s + 4)
+// of the input behind the Decimal(p + 10, s) buffer, bounded to 38.
+bool avg_result_type(const vr_agg_fn& f, int& rp, int& rs) {
+    if (f.result_precision > 0) {
+        rp = f.result_precision;
+        rs = f.result_scale;
+    } else {
+        if (f.precision >= 38) return false;
+        rp = std::min(f.precision - 6, 38);
+        rs = std::min(f.scale + 4, 38);
+    }
+    return rp >= 1 && rp <= 38 && rs >= f.scale && rs <= rp;
+}
+
+// Unsigned 256-bit integer for the average's division.
+struct U256 {
+    uint64_t w[4] = {0, 0, 0, 0};
+};
+bool u256_mul_small(U256& a, uint64_t m) {
+    u128 carry = 0;
+    for (int i = 0; i < 4; ++i) {
+        u128 p = (u128)a.w[i] * m + carry;
+        a.w[i] = (uint64_t)p;
+        carry = p >> 64;
+    }
+    return carry == 0;
+}
+void u256_add_small(U256& a, uint64_t v) {
+    u128 carry = v;
+    for (int i = 0; i < 4 && carry; ++i) {
+        u128 s = (u128)a.w[i] + carry;
+        a.w[i] = (uint64_t)s;
+        carry = s >> 64;
+    }
+}
+uint64_t u256_divmod_small(U256& a, uint64_t d) {
+    u128 rem = 0;
+    for (int i = 3; i >= 0; --i) {
+        u128 cur = (rem << 64) | a.w[i];
+        a.w[i] = (uint64_t)(cur / d);
+        rem = cur % d;
+    }
+    return (uint64_t)rem;
+}
+
+// Spark's Decimal./ as DecimalAvgResult evaluates it: BigDecimal(sum, ss)
+// .divide(BigDecimal(count), 39, HALF_UP).setScale(rs, HALF_UP), literally
+// in two roundings (VectorAggregates.scala:405-430). False when the result
+// reaches 10^rp.
+bool spark_decimal_avg(i128 sum, int64_t count, int ss, int rs, int rp, i128& out) {
+    const bool neg = sum < 0;
+    u128 mag = neg ? (u128)0 - (u128)sum : (u128)sum;
+    U256 n;
+    n.w[0] = (uint64_t)mag;
+    n.w[1] = (uint64_t)(mag >> 64);
+    for (int i = 0; i < 39 - ss; ++i)
+        if (!u256_mul_small(n, 10)) return false;
+    const uint64_t r = u256_divmod_small(n, (uint64_t)count);  // the quotient at scale 39
+    if (2 * (u128)r >= (u128)count) u256_add_small(n, 1);
+    const int m = 39 - rs;  // then to the result scale, half up
+    if (m > 0) {
+        U256 half;
+        half.w[0] = 5;
+        for (int i = 0; i < m - 1; ++i) u256_mul_small(half, 10);
+        u128 carry = 0;
+        for (int i = 0; i < 4; ++i) {
+            u128 s = (u128)n.w[i] + half.w[i] + carry;
+            n.w[i] = (uint64_t)s;
+            carry = s >> 64;
+        }
+        for (int i = 0; i < m; ++i) u256_divmod_small(n, 10);
+    }
+    if (n.w[2] || n.w[3]) return false;
+    u128 q = ((u128)n.w[1] << 64) | n.w[0];
+    if (q >= (u128)pow10_128(rp)) return false;
+    out = neg ? -(i128)q : (i128)q;
+    return true;
+}
+
 int build_outputs(orc_agg* a) {
     for (int32_t k : a->keys) {
         const vr_column_type& t = a->cols[k];
@@ -454,7 +533,13 @@ int build_outputs(orc_agg* a) {
                 break;
             case VR_FN_AVG_DECIMAL:
             case VR_FN_AVG_DECIMAL_MERGE:
-                add_out(a, VR_DECIMAL128, f.precision, f.scale);
+                if (f.flags & VR_FN_FINAL) {  // the result type: an INT64 lane up to 18 digits
+                    int rp, rs;
+                    if (!avg_result_type(f, rp, rs)) return fail(a, VR_ERR_INVALID, "decimal average result type");
+                    add_out(a, rp <= 18 ? VR_INT64 : VR_DECIMAL128, rp, rs);
+                } else {
+                    add_out(a, VR_DECIMAL128, f.precision, f.scale);
+                }
                 add_out(a, VR_INT64, 0, 0);
                 break;
             default: return fail(a, VR_ERR_UNSUPPORTED, "function kind");
@@ -498,6 +583,35 @@ Cell null_cell() {
     Cell c;
     c.valid = false;
     return c;
+}
+
+// One decimal average result: If(count = 0, null, DecimalDivideWithOverflowCheck(
+// sum, count, result type)): a null sum is null or ARITHMETIC_OVERFLOW (ANSI),
+// a result past its precision null or NUMERIC_VALUE_OUT_OF_RANGE (ANSI).
+int put_avg(orc_agg* a, const vr_out_column& out, int64_t o, const vr_agg_fn& f, int64_t count, bool sum_null,
+            i128 sum) {
+    int rp, rs;
+    avg_result_type(f, rp, rs);
+    const int lane = rp <= 18 ? VR_INT64 : VR_DECIMAL128;
+    const bool nullov = (f.flags & VR_FN_NULL_ON_OVERFLOW) != 0;
+    if (count == 0) {
+        put(out, lane, o, null_cell());
+        return VR_OK;
+    }
+    if (sum_null) {
+        if (!nullov) return fail(a, VR_ERR_DECIMAL_OVERFLOW, "overflow in sum of decimals");
+        put(out, lane, o, null_cell());
+        return VR_OK;
+    }
+    i128 q;
+    if (!spark_decimal_avg(sum, count, f.scale, rs, rp, q)) {
+        if (!nullov) return fail(a, VR_ERR_DECIMAL_PRECISION, "decimal precision");
+        put(out, lane, o, null_cell());
+        return VR_OK;
+    }
+    Cell c = dec_cell(q);
+    put(out, lane, o, c);
+    return VR_OK;
 }
 
 }  // namespace
@@ -605,8 +719,11 @@ int orc_agg_emit(orc_agg* a, int64_t from, int64_t to, const vr_out_column* outs
                     put(outs[j], VR_FLOAT64, o, s.count == 0 ? null_cell() : f64_cell(dval));
                     ++j;
                     break;
-                case VR_FN_AVG_DOUBLE: {  // AverageAgg: (sum, count), never null
-                    put(outs[j], VR_FLOAT64, o, f64_cell(dval));
+                case VR_FN_AVG_DOUBLE: {  // AverageAgg: (sum, count), never null; Complete: sum / count
+                    if (final_)
+                        put(outs[j], VR_FLOAT64, o, s.count == 0 ? null_cell() : f64_cell(dval / (double)s.count));
+                    else
+                        put(outs[j], VR_FLOAT64, o, f64_cell(dval));
                     Cell c;
                     c.lo = (uint64_t)s.count;
                     put(outs[j + 1], VR_INT64, o, c);
@@ -630,6 +747,15 @@ int orc_agg_emit(orc_agg* a, int64_t from, int64_t to, const vr_out_column* outs
                 case VR_FN_SUM_DECIMAL:
                 case VR_FN_AVG_DECIMAL: {  // WideDecimalSumAgg / WideDecimalAvgAgg buffers (:329-347, :374-389, :466-477)
                     i128 limit = pow10_128(f.precision);
+                    if (f.kind == VR_FN_AVG_DECIMAL && final_) {  // Complete: the average itself
+                        int rc = put_avg(a, outs[j], o, f, s.count, s.overflowed || abs128(s.wide) >= limit, s.wide);
+                        if (rc != VR_OK) return rc;
+                        Cell c2;
+                        c2.lo = (uint64_t)s.count;
+                        put(outs[j + 1], VR_INT64, o, c2);
+                        j += 2;
+                        break;
+                    }
                     bool past = s.overflowed || abs128(s.wide) >= limit;
                     Cell c;
                     if (s.count == 0) {
@@ -660,8 +786,11 @@ int orc_agg_emit(orc_agg* a, int64_t from, int64_t to, const vr_out_column* outs
                     ++j;
                     break;
                 }
-                case VR_FN_AVG_DOUBLE_MERGE: {
-                    put(outs[j], VR_FLOAT64, o, f64_cell(dval));
+                case VR_FN_AVG_DOUBLE_MERGE: {  // Final: sum / count, null for no rows
+                    if (final_)
+                        put(outs[j], VR_FLOAT64, o, s.count2 == 0 ? null_cell() : f64_cell(dval / (double)s.count2));
+                    else
+                        put(outs[j], VR_FLOAT64, o, f64_cell(dval));
                     Cell c;
                     c.lo = (uint64_t)s.count2;
                     put(outs[j + 1], VR_INT64, o, c);
@@ -691,8 +820,14 @@ int orc_agg_emit(orc_agg* a, int64_t from, int64_t to, const vr_out_column* outs
                 }
                 case VR_FN_AVG_DECIMAL_MERGE: {  // State.sum (VectorAggregates.scala:600-603)
                     i128 limit = pow10_128(f.precision);
-                    Cell c = (s.overflowed || abs128(s.wide) >= limit) ? null_cell() : dec_cell(s.wide);
-                    put(outs[j], VR_DECIMAL128, o, c);
+                    if (final_) {  // DecimalAvgResult; an ungrouped Final keeps a sum past the buffer precision
+                        bool past = s.overflowed || (!a->keys.empty() && abs128(s.wide) >= limit);
+                        int rc = put_avg(a, outs[j], o, f, s.count2, past, s.wide);
+                        if (rc != VR_OK) return rc;
+                    } else {
+                        Cell c = (s.overflowed || abs128(s.wide) >= limit) ? null_cell() : dec_cell(s.wide);
+                        put(outs[j], VR_DECIMAL128, o, c);
+                    }
                     Cell c2;
                     c2.lo = (uint64_t)s.count2;
                     put(outs[j + 1], VR_INT64, o, c2);

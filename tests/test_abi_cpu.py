@@ -83,10 +83,10 @@ def test_plan_composite_nullable_key_needs_two_words():
 def test_plan_refuses_what_the_gpu_gate_does_not_cover():
     cols = [vr.longs(np.zeros(1, np.int64), nullable=False), vr.decimals(np.zeros(1), 12, 2, nullable=False),
             vr.decimals(np.zeros(1), 12, 3, nullable=False)]
-    # a decimal average's result needs Spark's division: stays on the CPU path
-    f = vr.AggFunction(N.VR_FN_AVG_DECIMAL, 1, flags=N.VR_FN_FINAL, precision=22, scale=2)
+    # a 38-digit average buffer hides its input's precision: the result type must be given
+    f = vr.AggFunction(N.VR_FN_AVG_DECIMAL, 1, flags=N.VR_FN_FINAL, precision=38, scale=2)
     rc, info, _ = spec_of(cols, [0], [f]).plan()
-    assert rc == N.VR_ERR_UNSUPPORTED and b"division" in info.reason
+    assert rc == N.VR_ERR_INVALID and b"result type" in info.reason
     # a product whose scale needs rounding
     p = vr.DecimalProduct([(1, 1, 0), (2, 1, 0)])
     rc, info, _ = spec_of(cols, [0], [vr.WideDecimalSumAgg(p, 38, 4)]).plan()
@@ -95,6 +95,21 @@ def test_plan_refuses_what_the_gpu_gate_does_not_cover():
     cols2 = [vr.longs(np.zeros(1, np.int64), nullable=False), vr.bools(np.zeros(1, bool))]
     rc, info, _ = spec_of(cols2, [0], [vr.MinMaxAgg(1, True)]).plan()
     assert rc == N.VR_ERR_UNSUPPORTED
+
+
+def test_plan_types_final_averages_as_spark_does():
+    """Final / Complete averages: avg(double) a FLOAT64 result then the count;
+    avg(decimal(12,2)) over its Decimal(22,2) buffer a Decimal(16,6) result (an
+    INT64 lane up to 18 digits, DECIMAL128 beyond) then the count."""
+    cols = [vr.longs(np.zeros(1, np.int64), nullable=False), vr.decimals(np.zeros(1), 12, 2, nullable=False),
+            vr.doubles(np.zeros(1), nullable=False), vr.decimals128([0], 38, 2)]
+    fns = [vr.WideDecimalAvgAgg(1, 22, 2, final_result=True), vr.AverageAgg(2, final_result=True),
+           vr.WideDecimalAvgAgg(3, 38, 2, final_result=True, result_precision=38, result_scale=6)]
+    rc, info, outs = spec_of(cols, [0], fns).plan()
+    assert rc == N.VR_OK, info.reason
+    got = [(t.lane, t.precision, t.scale) for t in outs[1:]]
+    assert got == [(N.VR_INT64, 16, 6), (N.VR_INT64, 0, 0), (N.VR_FLOAT64, 0, 0), (N.VR_INT64, 0, 0),
+                   (N.VR_DECIMAL128, 38, 6), (N.VR_INT64, 0, 0)]
 
 
 def test_plan_too_many_accumulators_is_refused():

@@ -30,12 +30,15 @@ class AggFunction:
     scale: int = 0
     terms: Tuple[Tuple[int, int, int], ...] = ()  # (column, sign, addend)
     product_precision: int = 0
+    result_precision: int = 0  # final decimal average: result type (0 = Spark's from the buffer type)
+    result_scale: int = 0
 
     def to_ctypes(self) -> N.AggFn:
         f = N.AggFn()
         f.kind, f.input, f.input2, f.flags = self.kind, self.input, self.input2, self.flags
         f.precision, f.scale, f.num_terms = self.precision, self.scale, len(self.terms)
         f.product_precision = self.product_precision
+        f.result_precision, f.result_scale = self.result_precision, self.result_scale
         for i, (c, s, a) in enumerate(self.terms):
             f.terms[i] = N.Term(c, s, a)
         return f
@@ -56,9 +59,11 @@ def SumDoubleAgg(input: int, strict: bool = True) -> AggFunction:
     return AggFunction(N.VR_FN_SUM_DOUBLE, input, flags=N.VR_FN_STRICT if strict else 0)
 
 
-def AverageAgg(input: int, strict: bool = True) -> AggFunction:
-    """avg over doubles: buffer (sum, count) (VectorAggregates.scala:1021-1039)."""
-    return AggFunction(N.VR_FN_AVG_DOUBLE, input, flags=N.VR_FN_STRICT if strict else 0)
+def AverageAgg(input: int, strict: bool = True, final_result: bool = False) -> AggFunction:
+    """avg over doubles: buffer (sum, count) (VectorAggregates.scala:1021-1039);
+    `final_result` (Complete mode): the average itself, null for no rows, then the count."""
+    return AggFunction(N.VR_FN_AVG_DOUBLE, input,
+                       flags=(N.VR_FN_STRICT if strict else 0) | (N.VR_FN_FINAL if final_result else 0))
 
 
 def MinMaxAgg(input: int, is_min: bool) -> AggFunction:
@@ -89,12 +94,18 @@ def WideDecimalSumAgg(input, buffer_precision: int, scale: int, final_result: bo
     return AggFunction(N.VR_FN_SUM_DECIMAL, input, flags=flags, precision=buffer_precision, scale=scale)
 
 
-def WideDecimalAvgAgg(input, buffer_precision: int, scale: int) -> AggFunction:
-    """avg over a decimal: buffer (sum: Decimal(p+10, s), count) (VectorAggregates.scala:444-516)."""
+def WideDecimalAvgAgg(input, buffer_precision: int, scale: int, final_result: bool = False,
+                      null_on_overflow: bool = True, result_precision: int = 0, result_scale: int = 0) -> AggFunction:
+    """avg over a decimal: buffer (sum: Decimal(p+10, s), count) (VectorAggregates.scala:444-516);
+    `final_result` (Complete mode): DecimalAvgResult at Decimal(p+4, s+4) (or the given result
+    type), then the count (VectorAggregates.scala:405-430)."""
+    flags = (N.VR_FN_FINAL if final_result else 0) | (N.VR_FN_NULL_ON_OVERFLOW if null_on_overflow else 0)
     if isinstance(input, DecimalProduct):
-        return AggFunction(N.VR_FN_AVG_DECIMAL, -1, precision=buffer_precision, scale=scale,
-                           terms=tuple(input.factors), product_precision=input.precision)
-    return AggFunction(N.VR_FN_AVG_DECIMAL, input, precision=buffer_precision, scale=scale)
+        return AggFunction(N.VR_FN_AVG_DECIMAL, -1, flags=flags, precision=buffer_precision, scale=scale,
+                           terms=tuple(input.factors), product_precision=input.precision,
+                           result_precision=result_precision, result_scale=result_scale)
+    return AggFunction(N.VR_FN_AVG_DECIMAL, input, flags=flags, precision=buffer_precision, scale=scale,
+                       result_precision=result_precision, result_scale=result_scale)
 
 
 def CountMergeAgg(count: int) -> AggFunction:
@@ -102,9 +113,10 @@ def CountMergeAgg(count: int) -> AggFunction:
     return AggFunction(N.VR_FN_COUNT_MERGE, count)
 
 
-def AverageMergeAgg(sum_col: int, count_col: int) -> AggFunction:
-    """Final avg: (sum, count) buffers summed (VectorAggregates.scala:1065-1090)."""
-    return AggFunction(N.VR_FN_AVG_DOUBLE_MERGE, sum_col, count_col)
+def AverageMergeAgg(sum_col: int, count_col: int, final_result: bool = False) -> AggFunction:
+    """avg merge: (sum, count) buffers summed (VectorAggregates.scala:1065-1090); `final_result`:
+    Average's evaluateExpression, sum / count (null for no rows), then the count."""
+    return AggFunction(N.VR_FN_AVG_DOUBLE_MERGE, sum_col, count_col, flags=N.VR_FN_FINAL if final_result else 0)
 
 
 def WideDecimalSumMergeAgg(sum_col: int, is_empty_col: int, buffer_precision: int, scale: int,
@@ -114,9 +126,14 @@ def WideDecimalSumMergeAgg(sum_col: int, is_empty_col: int, buffer_precision: in
                        flags=_dec_flags(final_result, null_on_overflow), precision=buffer_precision, scale=scale)
 
 
-def WideDecimalAvgMergeAgg(sum_col: int, count_col: int, buffer_precision: int, scale: int) -> AggFunction:
-    """Merge of (sum, count) decimal average buffers (VectorAggregates.scala:526-642)."""
-    return AggFunction(N.VR_FN_AVG_DECIMAL_MERGE, sum_col, count_col, precision=buffer_precision, scale=scale)
+def WideDecimalAvgMergeAgg(sum_col: int, count_col: int, buffer_precision: int, scale: int,
+                           final_result: bool = False, null_on_overflow: bool = True, result_precision: int = 0,
+                           result_scale: int = 0) -> AggFunction:
+    """Merge of (sum, count) decimal average buffers (VectorAggregates.scala:526-642); `final_result`:
+    DecimalAvgResult in the sum slot (VectorAggregates.scala:405-430), then the count."""
+    flags = (N.VR_FN_FINAL if final_result else 0) | (N.VR_FN_NULL_ON_OVERFLOW if null_on_overflow else 0)
+    return AggFunction(N.VR_FN_AVG_DECIMAL_MERGE, sum_col, count_col, flags=flags, precision=buffer_precision,
+                       scale=scale, result_precision=result_precision, result_scale=result_scale)
 
 
 # --------------------------------------------------------------------- spec

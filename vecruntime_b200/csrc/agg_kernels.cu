@@ -146,6 +146,50 @@ VR_DEV double f64_total(const uint64_t* w) {
     return __dadd_rn(s, c);
 }
 
+// Spark's decimal average: |s| (a 128-bit magnitude at the sum's scale) over
+// a count, at a result scale `e` digits finer than the sum's: Decimal./
+// (BigDecimal.divide(divisor, 39, HALF_UP)) then setScale(rs, HALF_UP)
+// (DecimalAvgResult, VectorAggregates.scala:405-430). The quotient
+// q = |s| * 10^e / count is computed exactly (256 bits, remainder r); the
+// first rounding, at scale 39 (k = 39 - rs digits past the result scale),
+// can only move the second one when the fraction r / count lies within
+// 0.5 * 10^-k below one half: up <=> 10^k * (count - 2r) <= count, which for
+// k >= 20 needs 10^k <= count < 2^64 and so reduces to 2r >= count.
+// Returns false when the quotient leaves 128 bits (past any precision).
+VR_DEV bool dec_avg_magnitude(uint64_t lo, uint64_t hi, uint64_t count, int e, int k, uint64_t& qlo, uint64_t& qhi) {
+    uint64_t u[4] = {lo, hi, 0, 0};
+    for (int i = 0; i < e; ++i) {  // * 10^e, e <= 38
+        uint64_t carry = 0;
+        for (int j = 0; j < 4; ++j) {
+            const unsigned __int128 p = (unsigned __int128)u[j] * 10u + carry;
+            u[j] = (uint64_t)p;
+            carry = (uint64_t)(p >> 64);
+        }
+        if (carry) return false;
+    }
+    unsigned __int128 rem = 0;
+    for (int j = 3; j >= 0; --j) {  // / count, word by word
+        const unsigned __int128 cur = (rem << 64) | u[j];
+        u[j] = (uint64_t)(cur / count);
+        rem = cur % count;
+    }
+    const uint64_t r = (uint64_t)rem;
+    bool up = r >= count - r;  // 2r >= count
+    if (!up && k < 20) {
+        unsigned __int128 p10 = 1;
+        for (int i = 0; i < k; ++i) p10 *= 10u;
+        up = p10 * (unsigned __int128)(count - 2 * r) <= (unsigned __int128)count;
+    }
+    if (up) {
+        for (int j = 0; j < 4; ++j)
+            if (++u[j] != 0) break;
+    }
+    if (u[2] | u[3]) return false;
+    qlo = u[0];
+    qhi = u[1];
+    return true;
+}
+
 struct OutVal {
     uint64_t lo, hi;
     bool valid;
@@ -292,6 +336,72 @@ VR_DEV OutVal out_value(const Program& P, const OutDesc& od, const uint64_t* slo
             bool of;
             Wide t = op_total(OP_SUM_I64, acc + od.w0, of);
             r.lo = t.l[0];
+            break;
+        }
+        case OUT_AVG_DOUBLE: {
+            // Average's evaluateExpression: sum / count as doubles, null when
+            // no row counted (VectorAggregates.scala:1061-1064)
+            uint64_t cnt;
+            if (od.src_op == OP_SUM_I64) {
+                bool of;
+                cnt = op_total(OP_SUM_I64, acc + od.w1, of).l[0];
+            } else {
+                cnt = acc[od.w1];
+            }
+            if ((int64_t)cnt == 0) {
+                r.valid = false;
+                break;
+            }
+            r.lo = (uint64_t)__double_as_longlong(f64_total(acc + od.w0) / (double)(int64_t)cnt);
+            break;
+        }
+        case OUT_DEC_AVG: {
+            // If(count = 0, null, DecimalDivideWithOverflowCheck(sum, count, result type))
+            bool of = false, sum_null;
+            uint64_t cnt;
+            Wide t;
+            if (od.src_op == OP_MERGE_DAVG) {
+                t = op_total(OP_MERGE_DAVG, acc + od.w0, of);
+                cnt = op_total(OP_SUM_I64, acc + od.w1, of).l[0];
+                sum_null = (acc[od.w0 + 6] & kFlagOverflow) != 0;
+            } else {
+                cnt = (od.flags & OUTF_NULLCOUNT) ? acc[0] - acc[od.w1] : acc[od.w1];
+                if (od.src_op == OP_SUM_PROD && (acc[od.w0 + 6] & 1)) emit_error(ctrl, VR_ERR_DECIMAL_PRECISION);
+                t = op_total(od.src_op, acc + od.w0, of);
+                sum_null = of;
+            }
+            if ((int64_t)cnt == 0) {
+                r.valid = false;
+                break;
+            }
+            // the buffer's sum: null once it overflowed or past its precision
+            sum_null = sum_null || !wide_fits_i128(t) ||
+                       (!(od.flags & OUTF_UNGROUPED) && !within_precision(t.l[0], (int64_t)t.l[1], od.src_precision));
+            if (sum_null) {
+                r.valid = false;
+                if (!(od.flags & OUTF_NULL_ON_OVERFLOW)) emit_error(ctrl, VR_ERR_DECIMAL_OVERFLOW);
+                break;
+            }
+            const bool neg = (int64_t)t.l[1] < 0;
+            uint64_t mlo = t.l[0], mhi = t.l[1];
+            if (neg) {  // magnitude
+                mlo = ~mlo + 1;
+                mhi = ~mhi + (mlo == 0 ? 1 : 0);
+            }
+            uint64_t qlo, qhi;
+            const bool fits = dec_avg_magnitude(mlo, mhi, cnt, od.scale - od.src_scale, 39 - od.scale, qlo, qhi) &&
+                              (int64_t)qhi >= 0 && within_precision(qlo, (int64_t)qhi, od.precision);
+            if (!fits) {  // past the result precision: null, or NUMERIC_VALUE_OUT_OF_RANGE (ANSI)
+                r.valid = false;
+                if (!(od.flags & OUTF_NULL_ON_OVERFLOW)) emit_error(ctrl, VR_ERR_DECIMAL_PRECISION);
+                break;
+            }
+            if (neg) {
+                qlo = ~qlo + 1;
+                qhi = ~qhi + (qlo == 0 ? 1 : 0);
+            }
+            r.lo = qlo;
+            r.hi = qhi;
             break;
         }
     }

@@ -170,6 +170,24 @@ struct Builder {
         return o.word;
     }
 
+    OutDesc* last_out = nullptr;
+
+    // A decimal average's result type: given, or Spark's Decimal(p + 4, s + 4)
+    // of the input decimal(p, s) behind the Decimal(p + 10, s) buffer, bounded
+    // to 38 (Average.resultType; DecimalType.bounded).
+    int avg_result_type(const vr_agg_fn& f, int& rp, int& rs) {
+        if (f.result_precision > 0) {
+            rp = f.result_precision;
+            rs = f.result_scale;
+        } else {
+            if (f.precision >= 38) return fail(VR_ERR_INVALID, "a 38-digit average buffer needs its result type");
+            rp = std::min(f.precision - 10 + 4, 38);
+            rs = std::min(f.scale + 4, 38);
+        }
+        if (rp < 1 || rp > 38 || rs < f.scale || rs > rp) return fail(VR_ERR_UNSUPPORTED, "decimal average result type");
+        return VR_OK;
+    }
+
     void out(uint8_t kind, int lane, int flags, int src_op, int w0, int w1, int key, int precision, int scale) {
         EmitProgram& E = plan.emit;
         OutDesc& d = E.outs[E.num_out++];
@@ -183,6 +201,7 @@ struct Builder {
         d.key = (int8_t)key;
         d.precision = precision;
         d.scale = scale;
+        last_out = &d;
         vr_column_type t;
         std::memset(&t, 0, sizeof(t));
         t.lane = lane;
@@ -374,6 +393,9 @@ struct Builder {
                     int c = add_op(OP_COUNT_VALID, f.input, -1, 0, nullptr);
                     if (f.kind == VR_FN_SUM_DOUBLE) {
                         out(OUT_SUM_DOUBLE, VR_FLOAT64, 0, 0, w, c, -1, 0, 0);
+                    } else if (f.flags & VR_FN_FINAL) {  // Complete: the average itself, then the count
+                        out(OUT_AVG_DOUBLE, VR_FLOAT64, 0, 0, w, c, -1, 0, 0);
+                        out(OUT_COUNT, VR_INT64, 0, 0, c, 0, -1, 0, 0);
                     } else {
                         out(OUT_SUM_DOUBLE_NN, VR_FLOAT64, 0, 0, w, c, -1, 0, 0);
                         out(OUT_COUNT, VR_INT64, 0, 0, c, 0, -1, 0, 0);
@@ -401,8 +423,11 @@ struct Builder {
                 case VR_FN_SUM_DECIMAL:
                 case VR_FN_AVG_DECIMAL: {
                     if (f.precision < 1 || f.precision > 38) return fail(VR_ERR_INVALID, "decimal buffer precision");
-                    if (f.kind == VR_FN_AVG_DECIMAL && (f.flags & VR_FN_FINAL))
-                        return fail(VR_ERR_UNSUPPORTED, "decimal average result (division) stays on the CPU path");
+                    int rp = 0, rs = 0;
+                    if (f.kind == VR_FN_AVG_DECIMAL && (f.flags & VR_FN_FINAL)) {
+                        int rc2 = avg_result_type(f, rp, rs);
+                        if (rc2 != VR_OK) return rc2;
+                    }
                     int kind, w, c;
                     if (f.num_terms > 0) {
                         if (f.num_terms < 2 || f.num_terms > 3) return fail(VR_ERR_INVALID, "product needs 2 or 3 terms");
@@ -433,6 +458,12 @@ struct Builder {
                     if (f.kind == VR_FN_SUM_DECIMAL) {
                         out(OUT_DEC_SUM, VR_DECIMAL128, dflags | nc, kind, w, c, -1, f.precision, f.scale);
                         out(OUT_IS_EMPTY, VR_BOOL, nc, 0, 0, c, -1, 0, 0);
+                    } else if (f.flags & VR_FN_FINAL) {  // Complete: the average at its result type
+                        out(OUT_DEC_AVG, rp <= 18 ? VR_INT64 : VR_DECIMAL128,
+                            nc | ((f.flags & VR_FN_NULL_ON_OVERFLOW) ? OUTF_NULL_ON_OVERFLOW : 0), kind, w, c, -1, rp, rs);
+                        last_out->src_precision = (int16_t)f.precision;
+                        last_out->src_scale = (int16_t)f.scale;
+                        out(OUT_COUNT, VR_INT64, nc, 0, c, 0, -1, 0, 0);
                     } else {
                         out(OUT_DEC_SUM, VR_DECIMAL128, OUTF_ZERO_WHEN_EMPTY | nc, kind, w, c, -1, f.precision,
                             f.scale);
@@ -451,7 +482,10 @@ struct Builder {
                         return fail(VR_ERR_UNSUPPORTED, "avg merge needs (FLOAT64, INT64) buffers");
                     int ws = add_op(OP_SUM_F64, f.input, -1, 0, nullptr);
                     int wc = add_op(OP_SUM_I64, f.input2, -1, 0, nullptr);
-                    out(OUT_SUM_DOUBLE_NN, VR_FLOAT64, 0, 0, ws, 0, -1, 0, 0);
+                    if (f.flags & VR_FN_FINAL)  // Final: sum / count, null when no row counted
+                        out(OUT_AVG_DOUBLE, VR_FLOAT64, 0, OP_SUM_I64, ws, wc, -1, 0, 0);
+                    else
+                        out(OUT_SUM_DOUBLE_NN, VR_FLOAT64, 0, 0, ws, 0, -1, 0, 0);
                     out(OUT_SUM_LONG_NN, VR_INT64, 0, OP_SUM_I64, wc, 0, -1, 0, 0);
                     break;
                 }
@@ -469,11 +503,21 @@ struct Builder {
                 case VR_FN_AVG_DECIMAL_MERGE: {
                     if (!in || !in2 || in->lane != VR_DECIMAL128 || in2->lane != VR_INT64)
                         return fail(VR_ERR_UNSUPPORTED, "decimal avg merge needs (DECIMAL128, INT64) buffers");
-                    if (f.flags & VR_FN_FINAL)
-                        return fail(VR_ERR_UNSUPPORTED, "decimal average result (division) stays on the CPU path");
                     if (f.precision < 1 || f.precision > 38) return fail(VR_ERR_INVALID, "decimal buffer precision");
                     int w = add_op(OP_MERGE_DAVG, f.input, f.input2, 0, nullptr);
-                    out(OUT_DEC_MERGE, VR_DECIMAL128, 0, OP_MERGE_DAVG, w, 0, -1, f.precision, f.scale);
+                    if (f.flags & VR_FN_FINAL) {  // Final: DecimalAvgResult in the sum slot
+                        int rp = 0, rs = 0;
+                        int rc2 = avg_result_type(f, rp, rs);
+                        if (rc2 != VR_OK) return rc2;
+                        out(OUT_DEC_AVG, rp <= 18 ? VR_INT64 : VR_DECIMAL128,
+                            ((f.flags & VR_FN_NULL_ON_OVERFLOW) ? OUTF_NULL_ON_OVERFLOW : 0) |
+                                (spec.num_keys == 0 ? OUTF_UNGROUPED : 0),
+                            OP_MERGE_DAVG, w, w + 4, -1, rp, rs);
+                        last_out->src_precision = (int16_t)f.precision;
+                        last_out->src_scale = (int16_t)f.scale;
+                    } else {
+                        out(OUT_DEC_MERGE, VR_DECIMAL128, 0, OP_MERGE_DAVG, w, 0, -1, f.precision, f.scale);
+                    }
                     out(OUT_MERGE_COUNT, VR_INT64, 0, 0, w + 4, 0, -1, 0, 0);
                     break;
                 }

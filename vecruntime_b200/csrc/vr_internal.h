@@ -177,6 +177,11 @@ enum OutKind : uint8_t {
     OUT_IS_EMPTY,       // bool: count(w1)==0, or !nonEmpty flag (merge)
     OUT_DEC_MERGE,      // merged decimal sum (OP_MERGE_DSUM / OP_MERGE_DAVG) at w0
     OUT_MERGE_COUNT,    // int64 from carry-save count words of OP_MERGE_DAVG
+    OUT_AVG_DOUBLE,     // f64 pair at w0 divided by the count: carry-save words at w1
+                        //   (src_op OP_SUM_I64) or a count word (else); null for a zero count
+    OUT_DEC_AVG,        // decimal average: the sum as OUT_DEC_MERGE (src_op OP_MERGE_DAVG) or
+                        //   OUT_DEC_SUM (else, count word w1) reads it, over its count, at
+                        //   (precision, scale) from the sum's (src_precision, src_scale)
 };
 
 enum OutFlags : uint8_t {
@@ -187,6 +192,9 @@ enum OutFlags : uint8_t {
     OUTF_FROM_FLAGS = 16,      // OUT_IS_EMPTY from a merge flags word
     OUTF_ZERO_WHEN_EMPTY = 32, // decimal buffer: zero (valid) for an empty group
     OUTF_NULLCOUNT = 64,       // the count is rows (word 0) minus a null count word
+    OUTF_UNGROUPED = 128,      // OUT_DEC_AVG of a merge without grouping keys: the sum is not
+                               //   checked against the buffer precision (Spark's ungrouped Final
+                               //   keeps it in a local that nothing re-checks, VectorAggregates.scala:594-603)
 };
 
 struct OutDesc {
@@ -201,6 +209,8 @@ struct OutDesc {
     int8_t pad;
     int32_t precision;
     int32_t scale;
+    int16_t src_precision;  // OUT_DEC_AVG: the sum buffer's type
+    int16_t src_scale;
 };
 
 struct EmitProgram {

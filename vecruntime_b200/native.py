@@ -75,7 +75,8 @@ class Term(C.Structure):
 class AggFn(C.Structure):
     _fields_ = [("kind", C.c_int32), ("input", C.c_int32), ("input2", C.c_int32), ("flags", C.c_int32),
                 ("precision", C.c_int32), ("scale", C.c_int32), ("num_terms", C.c_int32),
-                ("product_precision", C.c_int32), ("terms", Term * 3)]
+                ("product_precision", C.c_int32), ("terms", Term * 3), ("result_precision", C.c_int32),
+                ("result_scale", C.c_int32)]
 
 
 class AggSpec(C.Structure):
