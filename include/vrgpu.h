@@ -85,9 +85,21 @@ typedef struct vr_column_type {
     int32_t scale;     /* decimal scale                                         */
     int32_t nullable;  /* 0: the column never carries a validity bitmap         */
     int32_t dict_size; /* VR_DICT32 / VR_BOOL keys: ids lie in [0, dict_size);
-                          0 = unknown (no direct indexing)                      */
-    int32_t reserved;
+                          0 = unknown (no direct indexing). With
+                          VR_COL_BATCH_DICTIONARY: the most distinct strings
+                          the table keeps for the column                        */
+    int32_t flags;     /* enum vr_column_flags                                  */
 } vr_column_type;
+
+enum vr_column_flags {
+    /* VR_DICT32 key whose batches each bring their own dictionary
+     * (vr_column.dictionary, e.g. Parquet row-group dictionaries): the
+     * handle maps every batch's entries onto a table dictionary it keeps
+     * across batches (GroupKeyTable.toIds, GroupKeyTable.java:1308-1430),
+     * keys are emitted as table ids, and vr_agg_key_dictionary returns the
+     * table dictionary's strings. A null entry makes its rows null. */
+    VR_COL_BATCH_DICTIONARY = 1
+};
 
 /* ---- aggregate functions (reference VectorAggFunction implementations) -- */
 enum vr_fn_kind {
@@ -283,6 +295,15 @@ int vr_agg_emit(vr_agg* h, int64_t from, int64_t to, const vr_out_column* outs, 
  *   settled first; the clear itself is queued on the handle's stream, ahead
  *   of later updates and emits, and does not wait for the device. */
 int vr_agg_reset(vr_agg* h);
+
+/* The table dictionary of key `key` (a VR_COL_BATCH_DICTIONARY key): the
+ * strings its emitted table ids stand for, in id order (GroupKeyTable's
+ * StringDictionary, GroupKeyTable.java:1308-1430; writeKeys emits them,
+ * :2851-2920). Writes *size; with `offsets` (size + 1 entries) and `data`
+ * (data_cap bytes) also the strings as an Arrow string array. *data_bytes
+ * receives the bytes needed. Host memory; no device work. */
+int vr_agg_key_dictionary(const vr_agg* h, int32_t key, int32_t* size, int32_t* offsets, uint8_t* data,
+                          int64_t data_cap, int64_t* data_bytes);
 
 /* Frees device state (GroupedAggState.close, VectorAggregates.scala:85-90). */
 void vr_agg_destroy(vr_agg* h);

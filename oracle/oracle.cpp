@@ -17,6 +17,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <string>
 #include <thread>
 #include <vector>
@@ -133,6 +134,10 @@ struct orc_agg {
     int64_t size = 0;
     int status = VR_OK;
     std::vector<vr_column_type> out_types;
+    // VR_COL_BATCH_DICTIONARY keys: the table dictionary (strings -> ids in
+    // first-use order, GroupKeyTable.toIds, GroupKeyTable.java:1308-1430)
+    std::vector<std::map<std::string, int32_t>> dict_ids;  // [key]
+    std::vector<std::vector<std::string>> dict_strings;   // [key][id]
 };
 
 namespace {
@@ -631,6 +636,8 @@ int orc_agg_create(const vr_agg_spec* spec, orc_agg** out) {
     a->slots.assign(2048, -1);  // INITIAL_CAPACITY * 2 (GroupKeyTable.java:574)
     a->mask = 2047;
     a->kvals.resize(a->keys.size());
+    a->dict_ids.resize(a->keys.size());
+    a->dict_strings.resize(a->keys.size());
     a->st.resize(a->fns.size());
     int rc = build_outputs(a);
     if (rc != VR_OK) {
@@ -641,9 +648,45 @@ int orc_agg_create(const vr_agg_spec* spec, orc_agg** out) {
     return VR_OK;
 }
 
+// Key k of row i; a key whose batches bring dictionaries becomes the table
+// id of its string (a null entry: a null key).
+KeyVal key_of(orc_agg* a, size_t k, const vr_batch& b, int64_t i) {
+    const vr_column_type& t = a->cols[a->keys[k]];
+    const vr_column& col = b.columns[a->keys[k]];
+    KeyVal kv = key_at(t, col, i);
+    if (!(t.flags & VR_COL_BATCH_DICTIONARY) || kv.null) return kv;
+    const vr_dictionary& d = *col.dictionary;
+    const int32_t e = (int32_t)kv.lo;
+    if (e < 0 || e >= d.size || (d.validity && !bit(d.validity, e))) {
+        kv.null = true;  // an id past the dictionary is refused by update; a null entry is a null key
+        kv.lo = 0;
+        return kv;
+    }
+    std::string s((const char*)d.data + d.offsets[e], (size_t)(d.offsets[e + 1] - d.offsets[e]));
+    auto& ids = a->dict_ids[k];
+    auto it = ids.find(s);
+    if (it == ids.end()) {
+        it = ids.emplace(s, (int32_t)ids.size()).first;
+        a->dict_strings[k].push_back(s);
+    }
+    kv.lo = (uint64_t)(uint32_t)it->second;
+    return kv;
+}
+
 int orc_agg_update(orc_agg* a, const vr_batch* b, int64_t chunk) {
     if (!a || !b) return VR_ERR_INVALID;
     if (a->status != VR_OK) return a->status;
+    for (size_t k = 0; k < a->keys.size(); ++k) {
+        const vr_column_type& t = a->cols[a->keys[k]];
+        if (!(t.flags & VR_COL_BATCH_DICTIONARY)) continue;
+        const vr_column& col = b->columns[a->keys[k]];
+        if (!col.dictionary) return fail(a, VR_ERR_INVALID, "a key declared with batch dictionaries came without one");
+        for (int64_t i = 0; i < b->num_rows; ++i) {
+            if (col.validity && !bit(col.validity, i)) continue;
+            const int32_t e = ((const int32_t*)col.data)[i];
+            if (e < 0 || e >= col.dictionary->size) return fail(a, VR_ERR_INVALID, "dictionary id outside its dictionary");
+        }
+    }
     const int64_t n = b->num_rows;
     if (chunk <= 0) chunk = n > 0 ? n : 1;
     std::vector<uint32_t> hashes((size_t)std::min(chunk, std::max<int64_t>(n, 1)));
@@ -656,12 +699,13 @@ int orc_agg_update(orc_agg* a, const vr_batch* b, int64_t chunk) {
         for (size_t k = 0; k < nk; ++k) {
             const vr_column_type& t = a->cols[a->keys[k]];
             const vr_column& col = b->columns[a->keys[k]];
-            for (int64_t r = 0; r < m; ++r) hashes[r] = mix32(hashes[r], key_hash_value(t.lane, key_at(t, col, c0 + r)));
+            (void)col;
+            for (int64_t r = 0; r < m; ++r) hashes[r] = mix32(hashes[r], key_hash_value(t.lane, key_of(a, k, *b, c0 + r)));
         }
         for (int64_t r = 0; r < m; ++r) {
             int64_t i = c0 + r;
             if (b->selection && !bit(b->selection, i)) continue;  // unselected rows create no group
-            for (size_t k = 0; k < nk; ++k) key[k] = key_at(a->cols[a->keys[k]], b->columns[a->keys[k]], i);
+            for (size_t k = 0; k < nk; ++k) key[k] = key_of(a, k, *b, i);
             int64_t g = nk == 0 ? (a->size == 0 ? new_group(a, 0, key) : 0) : lookup_or_insert(a, finish(hashes[r]), key);
             int rc = update_row(a, *b, i, g);
             if (rc != VR_OK) return rc;
@@ -844,8 +888,28 @@ int orc_agg_merge(orc_agg* dst, const orc_agg* src) {
     if (!dst || !src) return VR_ERR_INVALID;
     for (int64_t g = 0; g < src->size; ++g) {
         std::vector<KeyVal> key(src->keys.size());
-        for (size_t k = 0; k < key.size(); ++k) key[k] = src->kvals[k][g];
-        int64_t d = key.empty() ? (dst->size == 0 ? new_group(dst, 0, key) : 0) : lookup_or_insert(dst, src->ghash[g], key);
+        uint32_t h = src->ghash[g];
+        bool rehash = false;
+        for (size_t k = 0; k < key.size(); ++k) {
+            key[k] = src->kvals[k][g];
+            if ((src->cols[src->keys[k]].flags & VR_COL_BATCH_DICTIONARY) && !key[k].null) {
+                // the source's table id -> its string -> this table's id
+                const std::string& s = src->dict_strings[k][(size_t)key[k].lo];
+                auto it = dst->dict_ids[k].find(s);
+                if (it == dst->dict_ids[k].end()) {
+                    it = dst->dict_ids[k].emplace(s, (int32_t)dst->dict_ids[k].size()).first;
+                    dst->dict_strings[k].push_back(s);
+                }
+                key[k].lo = (uint64_t)(uint32_t)it->second;
+                rehash = true;
+            }
+        }
+        if (rehash) {
+            h = SEED;
+            for (size_t k = 0; k < key.size(); ++k) h = mix32(h, key_hash_value(src->cols[src->keys[k]].lane, key[k]));
+            h = finish(h);
+        }
+        int64_t d = key.empty() ? (dst->size == 0 ? new_group(dst, 0, key) : 0) : lookup_or_insert(dst, h, key);
         dst->rows[d] += src->rows[g];
         for (size_t fi = 0; fi < dst->fns.size(); ++fi) {
             FnState& a = dst->st[fi][d];
@@ -880,6 +944,25 @@ int orc_agg_merge(orc_agg* dst, const orc_agg* src) {
 }
 
 void orc_agg_destroy(orc_agg* a) { delete a; }
+
+int orc_agg_key_dictionary(const orc_agg* a, int32_t key, int32_t* size, int32_t* offsets, uint8_t* data,
+                           int64_t data_cap, int64_t* data_bytes) {
+    if (!a || !size || key < 0 || key >= (int32_t)a->keys.size()) return VR_ERR_INVALID;
+    const auto& strs = a->dict_strings[key];
+    *size = (int32_t)strs.size();
+    int64_t total = 0;
+    for (auto& s : strs) total += (int64_t)s.size();
+    if (data_bytes) *data_bytes = total;
+    if (data && data_cap < total) return VR_ERR_INVALID;
+    int64_t off = 0;
+    for (size_t i = 0; i < strs.size(); ++i) {
+        if (offsets) offsets[i] = (int32_t)off;
+        if (data) std::memcpy(data + off, strs[i].data(), strs[i].size());
+        off += (int64_t)strs[i].size();
+    }
+    if (offsets) offsets[strs.size()] = (int32_t)off;
+    return VR_OK;
+}
 const char* orc_last_error(void) { return g_err.c_str(); }
 
 int orc_hash_rows(int32_t nk, const vr_column_type* types, const vr_column* keys, int64_t n, uint32_t* out,

@@ -54,6 +54,11 @@ int orc_hash_rows(int32_t num_keys, const vr_column_type* types, const vr_column
 int orc_agg_run_threads(const vr_agg_spec* spec, const vr_batch* batch, int32_t threads, int64_t chunk_rows,
                         double* seconds, int64_t* groups);
 
+/* The strings behind key `key`'s emitted table ids (VR_COL_BATCH_DICTIONARY
+ * keys), as vr_agg_key_dictionary returns them. */
+int orc_agg_key_dictionary(const orc_agg* a, int32_t key, int32_t* size, int32_t* offsets, uint8_t* data,
+                           int64_t data_cap, int64_t* data_bytes);
+
 /* The same partitioned run folded into `dst` (the full-size parity check:
  * every group of the batch, ready for orc_agg_emit). */
 int orc_agg_update_threads(orc_agg* dst, const vr_batch* batch, int32_t threads, int64_t chunk_rows);

@@ -46,6 +46,8 @@ def lib():
         L.orc_agg_destroy.restype = None
         L.orc_last_error.restype = C.c_char_p
         L.orc_hash_rows.argtypes = [C.c_int32, C.POINTER(N.ColumnType), C.POINTER(N.Column), C.c_int64, P, C.c_int32]
+        L.orc_agg_key_dictionary.argtypes = [P, C.c_int32, C.POINTER(C.c_int32), P, P, C.c_int64,
+                                              C.POINTER(C.c_int64)]
         L.orc_agg_update_threads.argtypes = [P, C.POINTER(N.Batch), C.c_int32, C.c_int64]
         L.orc_agg_run_threads.argtypes = [C.POINTER(N.AggSpec), C.POINTER(N.Batch), C.c_int32, C.c_int64,
                                           C.POINTER(C.c_double), C.POINTER(C.c_int64)]
@@ -91,6 +93,16 @@ class Oracle:
 
     def num_groups(self) -> int:
         return lib().orc_agg_num_groups(self.h)
+
+    def key_dictionary(self, key: int):
+        """The strings (bytes) behind key `key`'s emitted table ids."""
+        n, nb = C.c_int32(), C.c_int64()
+        lib().orc_agg_key_dictionary(self.h, key, C.byref(n), None, None, 0, C.byref(nb))
+        offs = np.zeros(n.value + 1, np.int32)
+        data = np.zeros(max(1, nb.value), np.uint8)
+        lib().orc_agg_key_dictionary(self.h, key, C.byref(n), offs.ctypes.data, data.ctypes.data, nb.value,
+                                     C.byref(nb))
+        return [data[offs[i]:offs[i + 1]].tobytes() for i in range(n.value)]
 
     def emit(self, fp_mode: int = ORC_FP_COMPENSATED):
         from vecruntime_b200.aggregate import _out_arrays

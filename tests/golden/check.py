@@ -40,7 +40,7 @@ def inputs_digest(case) -> str:
     h = hashlib.sha256()
     for c in case.columns:
         t = c.ctype()
-        h.update(struct.pack("<6i", t.lane, t.precision, t.scale, t.nullable, t.dict_size, t.reserved))
+        h.update(struct.pack("<6i", t.lane, t.precision, t.scale, t.nullable, t.dict_size, t.flags))
     h.update(json.dumps([case.keys, [f.to_ctypes().kind for f in case.functions]]).encode())
     for b in case.batches:
         h.update(struct.pack("<q", b.num_rows))

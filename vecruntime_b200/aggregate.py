@@ -253,6 +253,18 @@ class GpuHashAggregate:
     def reset(self) -> None:
         N.check(self._lib.vr_agg_reset(self.h), "vr_agg_reset", self.h)
 
+    def key_dictionary(self, key: int):
+        """The strings (bytes) behind key `key`'s emitted table ids, when its
+        batches bring their own dictionaries (vr_agg_key_dictionary)."""
+        n, nb = C.c_int32(), C.c_int64()
+        N.check(self._lib.vr_agg_key_dictionary(self.h, key, C.byref(n), None, None, 0, C.byref(nb)),
+                "vr_agg_key_dictionary", self.h)
+        offs = np.zeros(n.value + 1, np.int32)
+        data = np.zeros(max(1, nb.value), np.uint8)
+        N.check(self._lib.vr_agg_key_dictionary(self.h, key, C.byref(n), offs.ctypes.data, data.ctypes.data,
+                                                nb.value, C.byref(nb)), "vr_agg_key_dictionary", self.h)
+        return [data[offs[i]:offs[i + 1]].tobytes() for i in range(n.value)]
+
     def stats(self) -> N.AggStats:
         st = N.AggStats()
         self._lib.vr_agg_get_stats(self.h, C.byref(st))

@@ -109,8 +109,11 @@ class Col:
         return len(self.data)
 
     def ctype(self) -> N.ColumnType:
+        """The column's type in a spec; a VR_DICT32 column that carries a
+        dictionary declares that its batches bring their own."""
         nullable = self.validity is not None if self.nullable is None else self.nullable
-        return N.ColumnType(self.lane, self.precision, self.scale, 1 if nullable else 0, self.dict_size, 0)
+        flags = N.VR_COL_BATCH_DICTIONARY if (self.lane == N.VR_DICT32 and self.dictionary is not None) else 0
+        return N.ColumnType(self.lane, self.precision, self.scale, 1 if nullable else 0, self.dict_size, flags)
 
 
 def _validity(nulls, n):
@@ -204,19 +207,25 @@ def host_batch(columns: List[Col], selection=None) -> HostBatch:
 
 @dataclass
 class DeviceBatch:
-    """Device-resident columns as raw device pointers (e.g. torch tensors' data_ptr)."""
+    """Device-resident columns as raw device pointers (e.g. torch tensors'
+    data_ptr); `dictionaries`: per column an N.Dictionary of device buffers, or None."""
     num_rows: int
     data_ptrs: List[int]
     validity_ptrs: List[Optional[int]]
     selection_ptr: Optional[int] = None
+    dictionaries: Optional[list] = None
     _keep: list = field(default_factory=list)
 
     def ctypes(self) -> N.Batch:
         arr = (N.Column * max(1, len(self.data_ptrs)))()
+        keep = [arr]
         for i, (d, v) in enumerate(zip(self.data_ptrs, self.validity_ptrs)):
             arr[i].data = d
             arr[i].validity = v
-        self._keep = [arr]
+            if self.dictionaries and self.dictionaries[i] is not None:
+                keep.append(self.dictionaries[i])
+                arr[i].dictionary = C.pointer(self.dictionaries[i])
+        self._keep = keep
         return N.Batch(self.num_rows, arr, self.selection_ptr, N.VR_DEVICE, 0)
 
 
@@ -243,4 +252,13 @@ def to_device(batch: HostBatch, device: int = 0):
     d = [put(c.data) for c in batch.columns]
     v = [put(c.validity) for c in batch.columns]
     s = put(batch.selection)
-    return DeviceBatch(batch.num_rows, d, v, s), tensors
+    dicts = None
+    if any(c.dictionary is not None for c in batch.columns):
+        dicts = []
+        for c in batch.columns:
+            if c.dictionary is None:
+                dicts.append(None)
+                continue
+            dd = c.dictionary
+            dicts.append(N.Dictionary(dd.size, 0, put(dd.offsets), put(dd.data), put(dd.validity), None))
+    return DeviceBatch(batch.num_rows, d, v, s, dicts), tensors

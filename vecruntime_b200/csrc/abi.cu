@@ -437,6 +437,13 @@ int agg_build(const vr_agg_spec* spec, const vr_tune_choice* forced, vr_agg** ou
         delete h;
         return rc;
     }
+    for (int k = 0; k < h->plan.prog.num_keys; ++k) {
+        if (!h->plan.prog.keys[k].remap) continue;
+        TableDict td;
+        td.key = k;
+        td.limit = h->columns[h->keys[k]].dict_size;
+        h->tdicts.push_back(std::move(td));
+    }
     cudaError_t e = cudaSetDevice(h->device);
     if (e != cudaSuccess) {
         set_thread_error(std::string("cudaSetDevice: ") + cudaGetErrorString(e));
@@ -798,6 +805,92 @@ const char* batch_nullability_error(const vr_agg* h, const vr_batch& b) {
     return nullptr;
 }
 
+// Maps the batch dictionary of every VR_COL_BATCH_DICTIONARY key onto the
+// key's table dictionary (one probe per dictionary entry, new strings get the
+// next table id; GroupKeyTable.toIds, GroupKeyTable.java:1308-1430) and points
+// the launch's descriptor at the maps, copied to the device on the handle's
+// stream ahead of the kernel. Dictionaries of device batches are read back
+// first (they are small next to the batch).
+static int map_batch_dictionaries(vr_agg* h, StageSlot& s, const vr_batch& b, BatchDesc& d) {
+    if (h->tdicts.empty()) return VR_OK;
+    int64_t need = 0;
+    for (const TableDict& td : h->tdicts) {
+        const vr_column& col = b.columns[h->spec.key_columns[td.key]];
+        if (!col.dictionary) return set_err(h, VR_ERR_INVALID, "a key declared with batch dictionaries came without one");
+        if (col.dictionary->size < 0) return set_err(h, VR_ERR_INVALID, "negative dictionary size");
+        need += col.dictionary->size;
+    }
+    cudaError_t e;
+    if (need > s.remap_cap) {
+        cudaFree(s.remap_dev);
+        cudaFreeHost(s.remap_host);
+        s.remap_dev = nullptr;
+        s.remap_host = nullptr;
+        s.remap_cap = 0;
+        const int64_t cap = std::max<int64_t>(need, 1024);
+        if ((e = cudaMalloc(&s.remap_dev, (size_t)cap * 4)) != cudaSuccess) return cuda_err(h, e, "dictionary maps");
+        if ((e = cudaMallocHost(&s.remap_host, (size_t)cap * 4)) != cudaSuccess) return cuda_err(h, e, "dictionary maps");
+        s.remap_cap = cap;
+    }
+    int64_t off = 0;
+    std::vector<int32_t> offs;
+    std::vector<uint8_t> bytes, valid;
+    for (TableDict& td : h->tdicts) {
+        const vr_dictionary& dict = *b.columns[h->spec.key_columns[td.key]].dictionary;
+        const int32_t n = dict.size;
+        const int32_t* o = dict.offsets;
+        const uint8_t* data = dict.data;
+        const uint8_t* vb = dict.validity;
+        if (n > 0 && (!o || !data)) return set_err(h, VR_ERR_INVALID, "dictionary without offsets or data");
+        if (n > 0 && b.location == VR_DEVICE) {  // read the device dictionary back
+            offs.resize((size_t)n + 1);
+            if ((e = cudaMemcpy(offs.data(), o, ((size_t)n + 1) * 4, cudaMemcpyDeviceToHost)) != cudaSuccess)
+                return cuda_err(h, e, "dictionary read-back");
+            bytes.resize((size_t)std::max(0, offs[n] - offs[0]) + 1);
+            if (offs[n] > offs[0] &&
+                (e = cudaMemcpy(bytes.data(), data + offs[0], (size_t)(offs[n] - offs[0]), cudaMemcpyDeviceToHost)) !=
+                    cudaSuccess)
+                return cuda_err(h, e, "dictionary read-back");
+            if (vb) {
+                valid.resize((size_t)(n + 7) / 8);
+                if ((e = cudaMemcpy(valid.data(), vb, valid.size(), cudaMemcpyDeviceToHost)) != cudaSuccess)
+                    return cuda_err(h, e, "dictionary read-back");
+                vb = valid.data();
+            }
+            for (int32_t k = n; k >= 0; --k) offs[k] -= offs[0];  // the bytes were read from offs[0] on
+            data = bytes.data();
+            o = offs.data();
+        }
+        int32_t* m = s.remap_host + off;
+        for (int32_t k = 0; k < n; ++k) {
+            if (vb && !((vb[k >> 3] >> (k & 7)) & 1)) {  // a null entry: its rows are null
+                m[k] = -1;
+                continue;
+            }
+            if (o[k + 1] < o[k]) return set_err(h, VR_ERR_INVALID, "dictionary offsets decrease");
+            std::string str(reinterpret_cast<const char*>(data + o[k]), (size_t)(o[k + 1] - o[k]));
+            auto it = td.ids.find(str);
+            if (it == td.ids.end()) {
+                const int32_t id = (int32_t)td.ids.size();
+                if (td.limit > 0 && id >= td.limit)
+                    return set_err(h, VR_ERR_INVALID, "more distinct strings than the key's declared dictionary size");
+                it = td.ids.emplace(str, id).first;
+                td.bytes += str;
+                td.offsets.push_back((int32_t)td.bytes.size());
+            }
+            m[k] = it->second;
+        }
+        const int c = h->plan.prog.keys[td.key].col;
+        d.col_remap[c] = s.remap_dev + off;
+        d.col_remap_n[c] = n;
+        off += n;
+    }
+    if (off > 0 && (e = cudaMemcpyAsync(s.remap_dev, s.remap_host, (size_t)off * 4, cudaMemcpyHostToDevice,
+                                        h->stream)) != cudaSuccess)
+        return cuda_err(h, e, "dictionary maps");
+    return VR_OK;
+}
+
 static int agg_update(vr_agg* h, const vr_batch* b) {
     if (h->dead) return VR_ERR_STATE;
     if (!b || b->num_rows < 0 || (b->num_rows > 0 && !b->columns))
@@ -852,6 +945,7 @@ static int agg_update(vr_agg* h, const vr_batch* b) {
     d.selection = sel;
     fill_desc(h, *b, d, s.ctrl_dev, s, 0);
     d.tma = tma_ok(h, d) ? 1 : 0;
+    if ((rc = map_batch_dictionaries(h, s, *b, d)) != VR_OK) return rc;
     *s.desc_host = d;
     s.launched = d;
     if ((e = cudaMemcpyAsync(s.desc_dev, s.desc_host, sizeof(BatchDesc), cudaMemcpyHostToDevice, h->stream)) != cudaSuccess)
@@ -1060,6 +1154,11 @@ int vr_agg_reset(vr_agg* h) {
     cudaError_t e = cudaMemsetAsync(h->table, 0, (size_t)h->table_slots * h->plan.prog.sw * 8, h->stream);
     if (e != cudaSuccess) return cuda_err(h, e, "reset");
     h->clear_queued = true;
+    for (TableDict& td : h->tdicts) {  // the emptied table's ids start again from 0
+        td.ids.clear();
+        td.offsets.assign(1, 0);
+        td.bytes.clear();
+    }
     h->groups_known = 0;
     h->compact_valid = false;
     h->num_groups = 0;
@@ -1079,6 +1178,8 @@ void vr_agg_destroy(vr_agg* h) {
         cudaFree(s.deferred);
         cudaFree(s.deferred_tmp);
         cudaFree(s.spill);
+        cudaFree(s.remap_dev);
+        cudaFreeHost(s.remap_host);
         if (s.done) cudaEventDestroy(s.done);
         if (s.t0) cudaEventDestroy(s.t0);
         if (s.t1) cudaEventDestroy(s.t1);
@@ -1121,6 +1222,27 @@ int vr_agg_last_error(const vr_agg* h, char* buf, size_t cap) {
 }
 
 const char* vr_thread_last_error(void) { return t_last_error.c_str(); }
+
+int vr_agg_key_dictionary(const vr_agg* h, int32_t key, int32_t* size, int32_t* offsets, uint8_t* data,
+                          int64_t data_cap, int64_t* data_bytes) {
+    if (!h || !size) return VR_ERR_INVALID;
+    for (const TableDict& td : h->tdicts) {
+        if (td.key != key) continue;
+        *size = (int32_t)td.ids.size();
+        if (data_bytes) *data_bytes = (int64_t)td.bytes.size();
+        if (offsets) std::memcpy(offsets, td.offsets.data(), td.offsets.size() * 4);
+        if (data) {
+            if (data_cap < (int64_t)td.bytes.size()) {
+                t_last_error = "vr_agg_key_dictionary: data buffer smaller than the dictionary's bytes";
+                return VR_ERR_INVALID;
+            }
+            std::memcpy(data, td.bytes.data(), td.bytes.size());
+        }
+        return VR_OK;
+    }
+    t_last_error = "vr_agg_key_dictionary: the key does not bring batch dictionaries";
+    return VR_ERR_INVALID;
+}
 
 const char* vr_status_string(int s) {
     switch (s) {

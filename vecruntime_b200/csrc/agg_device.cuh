@@ -363,7 +363,15 @@ struct TileView {
     const char* data[kMaxCols];
     const uint32_t* valid[kMaxCols];
     const uint32_t* sel;
+    const int32_t* remap[kMaxCols];  // VR_COL_BATCH_DICTIONARY keys: batch id -> table id
+    int32_t remap_n[kMaxCols];
 };
+
+// A key id through its batch dictionary's map: the table id, -1 for a null
+// entry, -2 for an id outside the batch dictionary.
+VR_DEV int32_t remap_id(const TileView& v, int c, uint32_t id) {
+    return id < (uint32_t)v.remap_n[c] ? v.remap[c][id] : -2;
+}
 
 VR_DEV bool bit_at(const uint32_t* words, int64_t r) { return (words[r >> 5] >> (r & 31)) & 1u; }
 VR_DEV bool col_valid(const TileView& v, int c, int64_t r) {
@@ -525,6 +533,18 @@ VR_DEV void pack_field(const KeyField& kf, const TileView& v, int64_t r, uint64_
         case VR_INT32:
         case VR_DICT32: {
             uint32_t u = (uint32_t)ld_i32(v, kf.col, r);
+            if (kf.remap) {  // the batch's dictionary id -> the table's
+                const int32_t t = remap_id(v, kf.col, u);
+                if (t == -1) {  // a null entry: the row's key is null (GroupKeyTable.java:1388-1389)
+                    if (kf.null_word >= 0)
+                        or_word<KW>(k, kf.null_word, 1ull << kf.null_shift);
+                    else
+                        bad = true;
+                    return;
+                }
+                if (t < 0) bad = true;
+                u = (uint32_t)(t < 0 ? 0 : t);
+            }
             if (kf.bits < 32 && (u >> kf.bits) != 0) bad = true;  // id outside the declared dictionary
             or_word<KW>(k, kf.word, (uint64_t)u << kf.shift);
             break;
@@ -578,6 +598,12 @@ VR_DEV int64_t direct_field(const KeyField& kf, const TileView& v, int64_t r) {
         val = bit_at(reinterpret_cast<const uint32_t*>(v.data[kf.col]), r);
     } else {
         val = (int64_t)(uint32_t)(SM ? lds32(v.data[kf.col], r) : ld_i32(v, kf.col, r));
+        if (kf.remap) {
+            const int32_t t = remap_id(v, kf.col, (uint32_t)val);
+            if (t == -1 && kf.null_word >= 0) return (int64_t)(kf.card - 1) * kf.mul;  // a null entry
+            if (t < 0) return -1;
+            val = t;
+        }
         if (val >= (int64_t)kf.card - (kf.null_word >= 0 ? 1 : 0)) return -1;
     }
     return val * kf.mul;
@@ -592,7 +618,12 @@ VR_DEV int direct_field32(const KeyField& kf, const TileView& v, int64_t r) {
     } else if (kf.lane == VR_BOOL) {
         val = (int)bit_at(reinterpret_cast<const uint32_t*>(v.data[kf.col]), r);
     } else {
-        const uint32_t id = (uint32_t)(SM ? lds32(v.data[kf.col], r) : ld_i32(v, kf.col, r));
+        uint32_t id = (uint32_t)(SM ? lds32(v.data[kf.col], r) : ld_i32(v, kf.col, r));
+        if (kf.remap) {
+            const int32_t t = remap_id(v, kf.col, id);
+            if (t == -1 && kf.null_word >= 0) return ((int)kf.card - 1) * (int)kf.mul;  // a null entry
+            id = t < 0 ? 0xffffffffu : (uint32_t)t;
+        }
         if (id >= (uint32_t)kf.card - (kf.null_word >= 0 ? 1u : 0u)) return -1;
         val = (int)id;
     }

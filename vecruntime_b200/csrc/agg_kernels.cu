@@ -43,6 +43,8 @@ __global__ void k_replay(const BatchDesc* __restrict__ desc, const int64_t* __re
     for (int c = 0; c < kMaxCols; ++c) {
         v.data[c] = D.col_data[c];
         v.valid[c] = D.col_valid[c];
+        v.remap[c] = D.col_remap[c];
+        v.remap_n[c] = D.col_remap_n[c];
     }
     v.sel = nullptr;
     uint32_t new_groups = 0;

@@ -117,6 +117,8 @@ VR_DEV void producer_loop(const Program& P, const BatchDesc* __restrict__ descs,
             const char* src = d.col_data[c] + (w ? row0 * w : row0 / 8);
             h.view.data[c] = bulk ? (const char*)(st + cfg.lay.data_off[c]) : src;
             bytes += bulk ? db : 0;
+            h.view.remap[c] = d.col_remap[c];
+            h.view.remap_n[c] = d.col_remap_n[c];
             const uint32_t* vsrc = d.col_valid[c] ? d.col_valid[c] + row0 / 32 : nullptr;
             if (vsrc && cfg.lay.valid_off[c] >= 0 && bulk) {
                 h.view.valid[c] = reinterpret_cast<const uint32_t*>(st + cfg.lay.valid_off[c]);

@@ -240,6 +240,11 @@ int vr_batched_create(const vr_batched_plan* plan, vr_batched** out) {
             set_thread_error("direct-tier batched instances must share their block shape");
             return VR_ERR_UNSUPPORTED;
         }
+        if (!h->tdicts.empty()) {
+            delete b;
+            set_thread_error("batched launches take table-level dictionary ids, not batch dictionaries");
+            return VR_ERR_UNSUPPORTED;
+        }
         if (vr_agg_sync(h) != VR_OK) {
             delete b;
             set_thread_error("instance handle failed");

@@ -142,7 +142,7 @@ std::string program_literal(const Program& P) {
     for (int k = 0; k < kMaxKeys; ++k) {
         const KeyField& f = P.keys[k];
         o << "{" << (int)f.col << "," << (int)f.lane << "," << (int)f.word << "," << (int)f.shift << "," << (int)f.bits
-          << "," << (int)f.null_word << "," << (int)f.null_shift << "," << (int)f.pad << "," << f.card << "," << f.pad2
+          << "," << (int)f.null_word << "," << (int)f.null_shift << "," << (int)f.remap << "," << f.card << "," << f.pad2
           << "," << (long long)f.mul << "LL}" << (k + 1 < kMaxKeys ? "," : "");
     }
     o << "}," << P.kw << "," << P.occ_word << "," << P.occ_shift << "," << P.lock_mode << "," << P.aw << "," << P.sw
@@ -165,7 +165,7 @@ std::string program_literal(const Program& P) {
 std::string key_literal(const KeyField& f) {
     std::ostringstream o;
     o << "{" << (int)f.col << "," << (int)f.lane << "," << (int)f.word << "," << (int)f.shift << "," << (int)f.bits << ","
-      << (int)f.null_word << "," << (int)f.null_shift << "," << (int)f.pad << "," << f.card << "," << f.pad2 << ","
+      << (int)f.null_word << "," << (int)f.null_shift << "," << (int)f.remap << "," << f.card << "," << f.pad2 << ","
       << (long long)f.mul << "LL}";
     return o.str();
 }

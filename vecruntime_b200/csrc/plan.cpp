@@ -321,6 +321,13 @@ struct Builder {
             P.occ_shift = 63;
         }
         if (P.kw > kMaxKW) return fail(VR_ERR_UNSUPPORTED, "grouping key wider than 256 bits");
+        // keys whose batches bring their own dictionaries go through a map to table ids
+        for (auto& f : fs) {
+            const vr_column_type& t = spec.columns[spec.key_columns[f.idx]];
+            if (!(t.flags & VR_COL_BATCH_DICTIONARY)) continue;
+            if (t.lane != VR_DICT32) return fail(VR_ERR_INVALID, "only VR_DICT32 keys bring batch dictionaries");
+            P.keys[f.idx].remap = 1;
+        }
         P.lock_mode = P.kw > 1 ? 1 : 0;
         // direct tier: combination multipliers
         if (direct) {

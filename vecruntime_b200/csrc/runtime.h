@@ -6,6 +6,7 @@
 
 #include <mutex>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "agg_kernels.cuh"
@@ -53,6 +54,20 @@ struct StageSlot {
     bool timed = false;
     bool staged_h2d = false;
     int64_t rows = 0;
+    int32_t* remap_dev = nullptr;   // batch dictionary -> table id maps of this batch
+    int32_t* remap_host = nullptr;  // pinned staging of those maps
+    int64_t remap_cap = 0;          // entries of both
+};
+
+// The strings of one VR_COL_BATCH_DICTIONARY key, in table-id order, and
+// their ids: every batch's dictionary is mapped onto it (GroupKeyTable's
+// StringDictionary, GroupKeyTable.java:1308-1430).
+struct TableDict {
+    int key = -1;                  // key index in the spec
+    int32_t limit = 0;             // the declared dict_size (0: no limit)
+    std::unordered_map<std::string, int32_t> ids;
+    std::vector<int32_t> offsets{0};
+    std::string bytes;
 };
 
 struct JitKernel;
@@ -119,6 +134,7 @@ struct vr_agg {
     vr::JitKernel* jit = nullptr;  // the spec's own kernel (owned by the process-wide cache)
     bool prebuilt_only = false;    // no per-spec kernel: blocks stay within the prebuilt kernel's bounds
     std::string jit_error;         // why it could not be compiled, when it could not
+    std::vector<vr::TableDict> tdicts;  // one per VR_COL_BATCH_DICTIONARY key
 };
 
 namespace vr {

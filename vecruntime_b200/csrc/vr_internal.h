@@ -86,7 +86,7 @@ struct KeyField {
     uint8_t bits;      // 1, 32, 64 or 128 (unsigned: 128 does not fit an int8_t)
     int8_t null_word;  // -1 when not nullable
     int8_t null_shift;
-    uint8_t pad;
+    uint8_t remap;     // 1: batches bring dictionaries; ids pass through TileView::remap
     int32_t card;      // direct tier: values of this field including null
     int32_t pad2;
     int64_t mul;       // direct tier: combination multiplier
@@ -135,6 +135,8 @@ struct BatchDesc {
     int32_t s_probes;        // hash tier: shared-memory probe limit (a table holding every
                              // group probes until it finds the key; a hot-key cache gives up soon)
     int32_t pad_;
+    const int32_t* col_remap[kMaxCols];  // batch dictionary id -> table id (-1: a null entry)
+    int32_t col_remap_n[kMaxCols];       // entries of each map (ids at or past it are bad keys)
 };
 
 // control block words

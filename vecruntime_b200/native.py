@@ -53,6 +53,8 @@ VR_SPEC_NO_TMA = 32
 VR_SPEC_TRACE = 64
 VR_SPEC_NO_JIT = 128
 
+VR_COL_BATCH_DICTIONARY = 1
+
 VR_HOST, VR_DEVICE = 0, 1
 VR_BATCHED_PERSISTENT, VR_BATCHED_PLAIN = 0, 1
 
@@ -65,7 +67,7 @@ class VrError(RuntimeError):
 
 class ColumnType(C.Structure):
     _fields_ = [("lane", C.c_int32), ("precision", C.c_int32), ("scale", C.c_int32),
-                ("nullable", C.c_int32), ("dict_size", C.c_int32), ("reserved", C.c_int32)]
+                ("nullable", C.c_int32), ("dict_size", C.c_int32), ("flags", C.c_int32)]
 
 
 class Term(C.Structure):
@@ -168,6 +170,8 @@ PROTOTYPES = [
     ("vr_agg_output_schema", C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(ColumnType), C.c_int32]),
     ("vr_agg_emit", C.c_int, [_P, C.c_int64, C.c_int64, C.POINTER(OutColumn), C.c_int32]),
     ("vr_agg_reset", C.c_int, [_P]),
+    ("vr_agg_key_dictionary", C.c_int, [_P, C.c_int32, C.POINTER(C.c_int32), _P, _P, C.c_int64,
+                                        C.POINTER(C.c_int64)]),
     ("vr_agg_destroy", None, [_P]),
     ("vr_agg_get_stats", C.c_int, [_P, C.POINTER(AggStats)]),
     ("vr_agg_last_error", C.c_int, [_P, C.c_char_p, C.c_size_t]),
