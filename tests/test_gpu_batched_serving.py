@@ -197,3 +197,28 @@ def test_serving_mix_equals_alone_and_the_oracle(cuda):
         assert 0 <= st.p99_wait_ms <= st.max_ms and 0 < st.p99_service_ms <= st.max_ms
     finally:
         srv.close()
+
+
+def test_serving_accounts_for_table_growth(cuda):
+    """A query whose table grows past its estimate holds more HBM: the
+    server's footprint follows the table, not the size it opened with."""
+    rng = np.random.default_rng(5)
+    rows = 200_000
+    cols = [Cc.longs(rng.integers(-(1 << 62), 1 << 62, rows, dtype=np.int64), nullable=False),
+            Cc.longs(rng.integers(0, 100, rows, dtype=np.int64), nullable=False),
+            Cc.doubles(rng.standard_normal(rows), nullable=False)]
+    w = G.Workload("grow", cols, [0], [A.CountAgg(), A.SumLongAgg(1), A.SumDoubleAgg(2)], 1024, rows)
+    srv = vr.AggregateServer(slots=4, hbm_cap_bytes=8 << 30)
+    try:
+        qid = srv.open_query(w.columns, w.keys, w.functions, est_groups=1024, max_batch_rows=20_000)
+        opened = srv.stats().hbm_in_use
+        tickets = [srv.submit(qid, w.batch(lo, lo + 20_000)) for lo in range(0, rows, 20_000)]
+        for t in tickets:
+            srv.wait(t)
+        types, arrays, n = srv.results(qid)
+        assert n == rows  # every key distinct: the table grew well past 1,024 groups
+        compare(w.spec(), types, arrays, n, *oracle_of(w, [w.batch()]))
+        st = srv.stats()
+        assert st.hbm_peak > opened + n * 16, (opened, st.hbm_peak)
+    finally:
+        srv.close()

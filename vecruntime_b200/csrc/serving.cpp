@@ -101,6 +101,14 @@ void CUDART_CB on_done(void* p) {
     delete a;
 }
 
+// A query's resident device bytes: its table (which grows as groups arrive)
+// plus both staging sets and deferred-row lists.
+int64_t query_bytes(const vr_agg* h) {
+    int64_t tb = h->table_slots * h->plan.prog.sw * 8;
+    for (const vr::StageSlot& sl : h->slot) tb += (int64_t)sl.dev_cap + sl.deferred_cap * 16;
+    return tb;
+}
+
 int64_t batch_bytes(const vr_agg* h, const vr_batch& b) {
     int64_t n = b.num_rows, bytes = 0;
     const vr::Program& P = h->plan.prog;
@@ -145,18 +153,24 @@ void dispatch_loop(vr_srv* s) {
             vr_agg* h = q.h;
             lk.unlock();
             int rc = vr_agg_update(h, &r->batch);
+            const int64_t now = query_bytes(h);  // the update may have grown the table
             CallbackArg* arg = new CallbackArg{s, r};
-            if (rc == VR_OK && cudaLaunchHostFunc(h->stream, on_done, arg) == cudaSuccess) {
-                lk.lock();
+            const bool ok = rc == VR_OK && cudaLaunchHostFunc(h->stream, on_done, arg) == cudaSuccess;
+            lk.lock();
+            // the query list may have grown (and moved) while the lock was released
+            Query& qn = s->queries[r->qid];
+            if (ok) {
+                s->table_bytes += now - qn.table_bytes;
+                qn.table_bytes = now;
+                s->st.hbm_peak = std::max(s->st.hbm_peak, s->table_bytes + s->in_flight_bytes);
             } else {
                 delete arg;
-                lk.lock();
                 r->status = rc == VR_OK ? VR_ERR_CUDA : rc;
                 r->state = 2;
                 r->t_done = Clock::now();
                 s->in_flight--;
                 s->in_flight_bytes -= r->bytes;
-                q.in_flight--;
+                qn.in_flight--;
                 s->done_cv.notify_all();
             }
             launched = true;
@@ -207,8 +221,7 @@ int vr_srv_open_query(vr_srv* s, const vr_agg_spec* spec, int32_t* query_id) {
         vr_agg_destroy(h);
         return rc;
     }
-    int64_t tb = h->table_slots * h->plan.prog.sw * 8;
-    for (const vr::StageSlot& sl : h->slot) tb += (int64_t)sl.dev_cap + sl.deferred_cap * 16;
+    const int64_t tb = query_bytes(h);
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->table_bytes + tb > s->cfg.hbm_cap_bytes) {
         vr_agg_destroy(h);
