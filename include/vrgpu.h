@@ -296,6 +296,14 @@ int vr_agg_emit(vr_agg* h, int64_t from, int64_t to, const vr_out_column* outs, 
  *   of later updates and emits, and does not wait for the device. */
 int vr_agg_reset(vr_agg* h);
 
+/* After vr_agg_emit returned VR_ERR_DECIMAL_PRECISION: the value that left
+ * its type (unscaled, lo and hi limbs) and that type, which Spark's
+ * NUMERIC_VALUE_OUT_OF_RANGE message names
+ * (VectorErrors.decimalPrecisionOverflow, VectorErrors.scala:71-73).
+ * VR_ERR_STATE when the emission recorded none (a total past 128 bits, or
+ * a product row past its precision). */
+int vr_agg_error_value(const vr_agg* h, int64_t* lo, int64_t* hi, int32_t* precision, int32_t* scale);
+
 /* The table dictionary of key `key` (a VR_COL_BATCH_DICTIONARY key): the
  * strings its emitted table ids stand for, in id order (GroupKeyTable's
  * StringDictionary, GroupKeyTable.java:1308-1430; writeKeys emits them,

@@ -79,6 +79,10 @@ def test_decimal_average_wide_result_and_its_errors(cuda):
             with pytest.raises(vr.VrError) as e:
                 agg.emit()
             assert e.value.status == status
+            if status == N.VR_ERR_DECIMAL_PRECISION:  # the value Spark's message names
+                assert agg.error_value() == (10 ** 34, 20, 6)
+            else:
+                assert agg.error_value() is None
         finally:
             agg.close()
 

@@ -253,6 +253,15 @@ class GpuHashAggregate:
     def reset(self) -> None:
         N.check(self._lib.vr_agg_reset(self.h), "vr_agg_reset", self.h)
 
+    def error_value(self):
+        """After a VR_ERR_DECIMAL_PRECISION emit: (unscaled value, precision,
+        scale) of the decimal that left its type, or None."""
+        lo, hi, p, s = C.c_int64(), C.c_int64(), C.c_int32(), C.c_int32()
+        if self._lib.vr_agg_error_value(self.h, C.byref(lo), C.byref(hi), C.byref(p), C.byref(s)) != N.VR_OK:
+            return None
+        u = ((hi.value & ((1 << 64) - 1)) << 64) | (lo.value & ((1 << 64) - 1))
+        return (u - (1 << 128) if u >> 127 else u), p.value, s.value
+
     def key_dictionary(self, key: int):
         """The strings (bytes) behind key `key`'s emitted table ids, when its
         batches bring their own dictionaries (vr_agg_key_dictionary)."""

@@ -1223,6 +1223,17 @@ int vr_agg_last_error(const vr_agg* h, char* buf, size_t cap) {
 
 const char* vr_thread_last_error(void) { return t_last_error.c_str(); }
 
+int vr_agg_error_value(const vr_agg* h, int64_t* lo, int64_t* hi, int32_t* precision, int32_t* scale) {
+    if (!h || !lo || !hi || !precision || !scale) return VR_ERR_INVALID;
+    const uint64_t ty = h->aux_ctrl_host ? h->aux_ctrl_host[CTRL_EMIT_VALUE_TYPE] : 0;
+    if (h->status != VR_ERR_DECIMAL_PRECISION || !(ty >> 63)) return VR_ERR_STATE;
+    *lo = (int64_t)h->aux_ctrl_host[CTRL_EMIT_VALUE_LO];
+    *hi = (int64_t)h->aux_ctrl_host[CTRL_EMIT_VALUE_HI];
+    *precision = (int32_t)((ty >> 32) & 0x7fffffff);
+    *scale = (int32_t)(uint32_t)ty;
+    return VR_OK;
+}
+
 int vr_agg_key_dictionary(const vr_agg* h, int32_t key, int32_t* size, int32_t* offsets, uint8_t* data,
                           int64_t data_cap, int64_t* data_bytes) {
     if (!h || !size) return VR_ERR_INVALID;

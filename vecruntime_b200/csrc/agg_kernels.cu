@@ -200,6 +200,17 @@ struct OutVal {
 VR_DEV void emit_error(uint64_t* ctrl, int status) {
     atomicCAS((unsigned long long*)&ctrl[CTRL_EMIT_ERROR], 0ull, (unsigned long long)status);
 }
+// The first error of an emission together with the offending value (a
+// decimal past its result type's precision), for Spark's message
+// (NUMERIC_VALUE_OUT_OF_RANGE names the value): the thread that sets the
+// status records it.
+VR_DEV void emit_error_value(uint64_t* ctrl, int status, uint64_t lo, uint64_t hi, int precision, int scale) {
+    if (atomicCAS((unsigned long long*)&ctrl[CTRL_EMIT_ERROR], 0ull, (unsigned long long)status) == 0ull) {
+        ctrl[CTRL_EMIT_VALUE_LO] = lo;
+        ctrl[CTRL_EMIT_VALUE_HI] = hi;
+        ctrl[CTRL_EMIT_VALUE_TYPE] = ((uint64_t)(uint32_t)precision << 32) | (uint32_t)scale | (1ull << 63);
+    }
+}
 
 VR_DEV OutVal out_value(const Program& P, const OutDesc& od, const uint64_t* slot, uint64_t* ctrl) {
     const uint64_t* acc = slot + P.kw;
@@ -292,8 +303,12 @@ VR_DEV OutVal out_value(const Program& P, const OutDesc& od, const uint64_t* slo
             bool past = of || !wide_fits_i128(t) || !within_precision(t.l[0], (int64_t)t.l[1], od.precision);
             if (past) {
                 r.valid = false;
-                if ((od.flags & OUTF_FINAL) && !(od.flags & OUTF_NULL_ON_OVERFLOW))
-                    emit_error(ctrl, VR_ERR_DECIMAL_PRECISION);
+                if ((od.flags & OUTF_FINAL) && !(od.flags & OUTF_NULL_ON_OVERFLOW)) {
+                    if (!of && wide_fits_i128(t))
+                        emit_error_value(ctrl, VR_ERR_DECIMAL_PRECISION, t.l[0], t.l[1], od.precision, od.scale);
+                    else
+                        emit_error(ctrl, VR_ERR_DECIMAL_PRECISION);
+                }
                 break;
             }
             r.lo = t.l[0];
@@ -327,7 +342,7 @@ VR_DEV OutVal out_value(const Program& P, const OutDesc& od, const uint64_t* slo
             if (!within_precision(t.l[0], (int64_t)t.l[1], od.precision)) {
                 r.valid = false;
                 if ((od.flags & OUTF_FINAL) && !(od.flags & OUTF_NULL_ON_OVERFLOW))
-                    emit_error(ctrl, VR_ERR_DECIMAL_PRECISION);
+                    emit_error_value(ctrl, VR_ERR_DECIMAL_PRECISION, t.l[0], t.l[1], od.precision, od.scale);
                 break;
             }
             r.lo = t.l[0];
@@ -391,16 +406,22 @@ VR_DEV OutVal out_value(const Program& P, const OutDesc& od, const uint64_t* slo
                 mhi = ~mhi + (mlo == 0 ? 1 : 0);
             }
             uint64_t qlo, qhi;
-            const bool fits = dec_avg_magnitude(mlo, mhi, cnt, od.scale - od.src_scale, 39 - od.scale, qlo, qhi) &&
-                              (int64_t)qhi >= 0 && within_precision(qlo, (int64_t)qhi, od.precision);
-            if (!fits) {  // past the result precision: null, or NUMERIC_VALUE_OUT_OF_RANGE (ANSI)
-                r.valid = false;
-                if (!(od.flags & OUTF_NULL_ON_OVERFLOW)) emit_error(ctrl, VR_ERR_DECIMAL_PRECISION);
-                break;
-            }
-            if (neg) {
+            const bool q128 = dec_avg_magnitude(mlo, mhi, cnt, od.scale - od.src_scale, 39 - od.scale, qlo, qhi) &&
+                              (int64_t)qhi >= 0;
+            if (q128 && neg) {
                 qlo = ~qlo + 1;
                 qhi = ~qhi + (qlo == 0 ? 1 : 0);
+            }
+            if (!q128 || !within_precision(qlo, (int64_t)qhi, od.precision)) {
+                // past the result precision: null, or NUMERIC_VALUE_OUT_OF_RANGE (ANSI)
+                r.valid = false;
+                if (!(od.flags & OUTF_NULL_ON_OVERFLOW)) {
+                    if (q128)
+                        emit_error_value(ctrl, VR_ERR_DECIMAL_PRECISION, qlo, qhi, od.precision, od.scale);
+                    else
+                        emit_error(ctrl, VR_ERR_DECIMAL_PRECISION);
+                }
+                break;
             }
             r.lo = qlo;
             r.hi = qhi;

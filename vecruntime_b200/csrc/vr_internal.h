@@ -148,7 +148,11 @@ enum Ctrl : int {
     CTRL_TIMEOUT_WHERE = 4,
     CTRL_EMIT_ERROR = 5,  // emission status (VR_ERR_*)
     CTRL_SPILLED = 6,     // slots appended to the spill list
-    CTRL_WORDS = 8
+    CTRL_WORDS = 8,
+    // an emission's control block: the value behind its first error
+    CTRL_EMIT_VALUE_LO = 2,
+    CTRL_EMIT_VALUE_HI = 3,
+    CTRL_EMIT_VALUE_TYPE = 4,  // bit 63: recorded; precision << 32 | scale
 };
 constexpr uint64_t kErrTimeout = 1;
 constexpr uint64_t kErrDeferredFull = 2;

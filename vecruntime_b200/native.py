@@ -170,6 +170,8 @@ PROTOTYPES = [
     ("vr_agg_output_schema", C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(ColumnType), C.c_int32]),
     ("vr_agg_emit", C.c_int, [_P, C.c_int64, C.c_int64, C.POINTER(OutColumn), C.c_int32]),
     ("vr_agg_reset", C.c_int, [_P]),
+    ("vr_agg_error_value", C.c_int, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int32),
+                                     C.POINTER(C.c_int32)]),
     ("vr_agg_key_dictionary", C.c_int, [_P, C.c_int32, C.POINTER(C.c_int32), _P, _P, C.c_int64,
                                         C.POINTER(C.c_int64)]),
     ("vr_agg_destroy", None, [_P]),
