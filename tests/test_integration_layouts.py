@@ -63,7 +63,7 @@ def test_ctypes_mirrors_match_the_header(tmp_path):
         pytest.skip("no C compiler")
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "vrgpu.h"', "int main(void) {"]
     for key, cname in C_NAMES.items():
-        lines.append(f'printf("{key} size %zu\\n", sizeof({cname}));')
+        lines.append(f'printf("{key} @sizeof %zu\\n", sizeof({cname}));')
         for f in MIRRORS[key]._fields_:
             lines.append(f'printf("{key} {f[0]} %zu\\n", offsetof({cname}, {f[0]}));')
     lines.append("return 0; }")
@@ -75,5 +75,5 @@ def test_ctypes_mirrors_match_the_header(tmp_path):
     for ln in filter(None, out):
         key, field, value = ln.split()
         mirror = MIRRORS[key]
-        want = C.sizeof(mirror) if field == "size" else getattr(mirror, field).offset
+        want = C.sizeof(mirror) if field == "@sizeof" else getattr(mirror, field).offset
         assert int(value) == want, (key, field, value, want)
