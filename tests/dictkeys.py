@@ -33,7 +33,9 @@ def dictionary_batches(seed, batches=4, rows=5000, null_rows=0.05, dict_size=0):
 def canonical(arrays, n, key, strings):
     """The emitted arrays with key column `key`'s table ids replaced by the
     position of their string in the sorted word list (nulls stay null)."""
-    universe = sorted(set(w.encode() for w in WORDS) | set(strings))
+    # one universe for both sides: a table may hold strings no row used (the
+    # GPU maps every entry of a batch dictionary, the oracle the ones rows use)
+    universe = sorted(set(w.encode() for w in WORDS) | {b"unused-%d" % b for b in range(64)} | set(strings))
     rank = {s: i for i, s in enumerate(universe)}
     ids = arrays[key][0][:n]
     mapped = np.array([rank[strings[int(i)]] for i in ids], np.int32) if n else np.zeros(0, np.int32)
