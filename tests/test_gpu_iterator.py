@@ -31,9 +31,13 @@ COMPLETE = [A.CountAgg(), A.CountAgg(1), A.SumLongAgg(1), A.MinMaxAgg(1, True), 
 
 
 def rows_of_keys(seed, rows, groups, batch=8192):
+    """`rows` rows over `groups` distinct int64 keys (groups=None: every row its own key)."""
     rng = np.random.default_rng(seed)
-    domain = rng.integers(-(1 << 62), 1 << 62, groups, dtype=np.int64)
-    k = domain[rng.integers(0, groups, rows)]
+    if groups is None:
+        k = rng.permutation(rows).astype(np.int64) * 7919 + 13
+    else:
+        domain = rng.integers(-(1 << 62), 1 << 62, groups, dtype=np.int64)
+        k = domain[rng.integers(0, groups, rows)]
     v1 = rng.integers(-10 ** 6, 10 ** 6, rows, dtype=np.int64)
     nulls = rng.random(rows) < 0.05
     v2 = rng.standard_normal(rows)
@@ -95,7 +99,7 @@ def test_emit_and_reset_past_the_budget(cuda):
 
 
 def test_pass_through_when_the_input_does_not_reduce(cuda):
-    cols, batches = rows_of_keys(2, 100_000, 10 ** 12)  # every row its own group
+    cols, batches = rows_of_keys(2, 100_000, None)  # every row its own group
     it = I.GpuGroupedAggregateIterator(batches, cols, [0], PARTIAL,
                                        policy=I.EmitAndReset(256 << 10, pass_through_ratio=2.0), est_groups=1024,
                                        max_batch_rows=8192)
