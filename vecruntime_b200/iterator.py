@@ -106,16 +106,16 @@ class AggregateMemory:
             self.reserved = 0
 
 
-def _take(t: N.ColumnType, data, validity, n, idx) -> Col:
-    """Rows `idx` of an emitted column as a new input column."""
-    valid = unpack_bits(validity, n)[idx]
+def _take(t: N.ColumnType, data, validity, n, idx, nullable: bool) -> Col:
+    """Rows `idx` of an emitted column as a new input column (with a validity
+    bitmap only when the input column it feeds is nullable)."""
+    valid = pack_bits(unpack_bits(validity, n)[idx]) if nullable else None
     if t.lane == N.VR_BOOL:
         vals = unpack_bits(data, n)[idx]
-        c = Col(t.lane, pack_bits(vals), pack_bits(valid), t.precision, t.scale, t.dict_size, True)
+        c = Col(t.lane, pack_bits(vals), valid, t.precision, t.scale, t.dict_size, nullable)
         c._n = len(idx)
         return c
-    return Col(t.lane, np.ascontiguousarray(data[:n][idx]), pack_bits(valid), t.precision, t.scale, t.dict_size,
-               True)
+    return Col(t.lane, np.ascontiguousarray(data[:n][idx]), valid, t.precision, t.scale, t.dict_size, nullable)
 
 
 class GpuGroupedAggregateIterator:
@@ -209,11 +209,12 @@ class GpuGroupedAggregateIterator:
             return
         arrays = self.agg.emit()
         b = self._buckets_of(arrays, n, len(spill))
+        nullable = [bool(c.ctype().nullable) for c in self.columns]
         for k in range(len(spill)):
             idx = np.flatnonzero(b == k)
             if len(idx):
-                spill[k].append(HostBatch([_take(t, d, v, n, idx) for t, (d, v) in zip(self.output_types, arrays)],
-                                          len(idx)))
+                spill[k].append(HostBatch([_take(t, d, v, n, idx, nl) for t, (d, v), nl in
+                                           zip(self.output_types, arrays, nullable)], len(idx)))
 
     # ------------------------------------------------------------ driving
     def __iter__(self):
