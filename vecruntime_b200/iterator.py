@@ -138,8 +138,9 @@ class GpuGroupedAggregateIterator:
         self.tables_emitted = 0  # tables that went out before the input ended (spills / emit-and-reset)
         self.fill_rows = 0
         self.device = device
+        self._types = [c.ctype() if isinstance(c, Col) else c for c in self.columns]
         if isinstance(self.policy, GraceHash):
-            types = [c.ctype() for c in self.columns]
+            types = self._types
             if self.keys != list(range(len(self.keys))) or \
                     [t.lane for t in self.output_types] != [t.lane for t in types] or \
                     any(f.flags & N.VR_FN_FINAL for f in functions):
@@ -209,7 +210,7 @@ class GpuGroupedAggregateIterator:
             return
         arrays = self.agg.emit()
         b = self._buckets_of(arrays, n, len(spill))
-        nullable = [bool(c.ctype().nullable) for c in self.columns]
+        nullable = [bool(t.nullable) for t in self._types]
         for k in range(len(spill)):
             idx = np.flatnonzero(b == k)
             if len(idx):
