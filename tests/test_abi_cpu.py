@@ -199,3 +199,21 @@ def test_plan_shares_accumulators_between_functions():
     types = (N.ColumnType * 64)()
     assert N.lib().vr_agg_plan(C.byref(sp.spec), C.byref(info), types, 64) == N.VR_OK
     assert info.num_ops == 6 and info.direct_ok == 1
+
+
+def test_tuner_key_tells_apart_specs_that_differ_only_in_types_or_flags():
+    """Two specs that differ only in a decimal precision, a function flag or
+    a product term get separate tuner entries."""
+    lib = N.lib()
+    cols = [vr.longs(np.zeros(1, np.int64), nullable=False), vr.decimals(np.zeros(1), 12, 2, nullable=False)]
+    base = vr.Spec(cols, [0], [vr.WideDecimalSumAgg(1, 22, 2)])
+    other_prec = vr.Spec(cols, [0], [vr.WideDecimalSumAgg(1, 23, 2)])
+    other_flag = vr.Spec(cols, [0], [vr.WideDecimalSumAgg(1, 22, 2, null_on_overflow=False)])
+    rows = 5_000_011
+    t = N.TuneChoice()
+    t.tier, t.threads, t.tile_rows = 2, 128, 512
+    assert lib.vr_tune_record(C.byref(base.spec), rows, C.byref(t), C.c_double(1e9)) == N.VR_OK
+    out = N.TuneChoice()
+    assert lib.vr_tune_lookup(C.byref(base.spec), rows, C.byref(out)) == 1
+    assert lib.vr_tune_lookup(C.byref(other_prec.spec), rows, C.byref(out)) == 0
+    assert lib.vr_tune_lookup(C.byref(other_flag.spec), rows, C.byref(out)) == 0

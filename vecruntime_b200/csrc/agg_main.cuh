@@ -61,8 +61,10 @@ VR_DEV int find_instance(const BatchDesc* descs, int n, int64_t t) {
     return lo;
 }
 
-// The producer thread: fetches tile indices (one ahead, so the atomic's round
-// trip overlaps the previous tile's issue), finds the tile's instance with a
+// The producer thread: takes tiles from the work counter in runs of
+// cfg.tile_run consecutive tiles (the next run is fetched while the last tile
+// of the current one is issued, so the atomic's round trip overlaps it),
+// finds the tile's instance with a
 // cursor that only moves forward (a producer's tile indices only grow), keeps
 // that instance's descriptor in its own shared-memory copy (reloaded only
 // when the instance changes), and issues the tile's bulk copies.
@@ -73,7 +75,9 @@ VR_DEV void producer_loop(const Program& P, const BatchDesc* __restrict__ descs,
     const int T = cfg.tile_rows;
     if (cfg.test_stall) return;  // test hook: nothing issued, nothing in flight
     int cur = -1;
-    int64_t t_next = (int64_t)atomicAdd((unsigned long long*)tile_counter, 1ull);
+    const uint64_t run_len = cfg.tile_run > 1 ? (uint64_t)cfg.tile_run : 1ull;
+    int64_t run = (int64_t)atomicAdd((unsigned long long*)tile_counter, run_len);
+    uint64_t taken = 0;
     // the stage index and its barrier phase advance with each tile (a 64-bit
     // division by the run-time stage count per tile costs more than the tile's
     // own bookkeeping)
@@ -82,14 +86,17 @@ VR_DEV void producer_loop(const Program& P, const BatchDesc* __restrict__ descs,
             set_error(descs[0].ctrl, kErrTimeout);
             return;
         }
-        const int64_t t = t_next;
+        const int64_t t = run + (int64_t)taken;
         StageHdr& h = hdr[s];
         if (t >= cfg.total_tiles) {
             h.tile = -1;
             mbar_arrive(&full[s]);
             return;
         }
-        t_next = (int64_t)atomicAdd((unsigned long long*)tile_counter, 1ull);
+        if (++taken == run_len) {  // the run is used up: fetch the next one now
+            run = (int64_t)atomicAdd((unsigned long long*)tile_counter, run_len);
+            taken = 0;
+        }
         int inst = cur < 0 ? 0 : cur;
         if (cfg.num_desc > 1)
             while (inst + 1 < cfg.num_desc && descs[inst + 1].tile_begin <= t) ++inst;

@@ -27,7 +27,8 @@ struct LaunchCfg {
     int32_t rchunk;            // rows per consumer thread per chunk: 2, 4 or 8 (direct), 1 (hash)
     int32_t wait_polls;        // bounded barrier waits: suspended polls of up to 1 ms before giving up
     int32_t test_stall;        // test hook: the producer leaves at once, so consumer waits run out
-    int32_t pad;
+    int32_t tile_run;          // tiles a producer takes per grab from the work counter (1 or more):
+                               // consecutive tiles, so fewer CTAs touch each small instance
     StageLayout lay;
 };
 

@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -105,6 +106,11 @@ static int batched_enqueue(vr_batched* b, cudaStream_t st) {
     return VR_OK;
 }
 
+// Tiles a producer takes per grab in the persistent launch: consecutive tiles
+// of one instance, so a small instance is spread over fewer CTAs (each of
+// which flushes its shared-memory table into the instance's HBM table).
+constexpr int kBatchedTileRun = 8;
+
 // The persistent launch's block shape (hash tier): one for every instance,
 // since the stage layout and the kernel's thread count are per launch.
 // Measured defaults: two CTAs per SM of 256 consumer threads, 512-row tiles
@@ -133,6 +139,8 @@ static int batched_shape(vr_batched* b, const vr_tune_choice* shape) {
     while (area * 2 * 8 * P.sw <= budget - base) area *= 2;  // power-of-two tables
     LaunchCfg& L = b->cfg;
     L = h0->launch;
+    L.tile_run = kBatchedTileRun;
+    if (const char* e = std::getenv("VRGPU_TILE_RUN")) L.tile_run = std::max(1, std::atoi(e));
     L.tile_rows = T;
     L.stages = stages;
     L.consumer_threads = threads;

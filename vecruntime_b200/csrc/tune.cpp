@@ -43,18 +43,28 @@ uint64_t fnv(uint64_t h, uint64_t v) {
 
 }  // namespace
 
+// Everything in a spec that changes the kernel or its cost: column lanes,
+// nullability, dictionary sizes, decimal types and flags, the keys, and every
+// function field (kind, inputs, flags, types, product terms and precision).
 uint64_t spec_signature(const vr_agg_spec& s) {
     uint64_t h = 0xcbf29ce484222325ull;
     h = fnv(h, (uint64_t)s.num_columns);
     for (int c = 0; c < s.num_columns; ++c) {
-        h = fnv(h, (uint64_t)s.columns[c].lane | ((uint64_t)s.columns[c].nullable << 8) |
-                       ((uint64_t)(uint32_t)s.columns[c].dict_size << 16));
+        const vr_column_type& t = s.columns[c];
+        h = fnv(h, (uint64_t)t.lane | ((uint64_t)t.nullable << 8) | ((uint64_t)(uint32_t)t.dict_size << 16));
+        h = fnv(h, (uint64_t)(uint32_t)t.precision | ((uint64_t)(uint32_t)t.scale << 16) | ((uint64_t)(uint32_t)t.flags << 32));
     }
     for (int k = 0; k < s.num_keys; ++k) h = fnv(h, (uint64_t)s.key_columns[k] + 1000);
     for (int f = 0; f < s.num_fns; ++f) {
         const vr_agg_fn& fn = s.fns[f];
         h = fnv(h, (uint64_t)fn.kind | ((uint64_t)(uint32_t)fn.input << 8) | ((uint64_t)(uint32_t)fn.input2 << 24) |
                        ((uint64_t)fn.num_terms << 40));
+        h = fnv(h, (uint64_t)(uint32_t)fn.flags | ((uint64_t)(uint32_t)fn.precision << 16) |
+                       ((uint64_t)(uint32_t)fn.scale << 32) | ((uint64_t)(uint32_t)fn.product_precision << 48));
+        h = fnv(h, (uint64_t)(uint32_t)fn.result_precision | ((uint64_t)(uint32_t)fn.result_scale << 32));
+        for (int t = 0; t < fn.num_terms && t < 3; ++t)
+            h = fnv(h, ((uint64_t)(uint32_t)fn.terms[t].column | ((uint64_t)(uint32_t)fn.terms[t].sign << 32)) ^
+                           (uint64_t)fn.terms[t].addend);
     }
     return h;
 }
