@@ -506,16 +506,30 @@ def run_batched(args, rank, world, device, check):
     rows = sum(w.rows for w in ws)
     in_bytes = sum(G.input_bytes(w) for w in ws)
     log(f"[rank {rank}] batched: {len(ws)} instances, {rows} rows, {sum(w.est_groups for w in ws)} est groups")
-    aggs, dbs, keep = [], [], []
+    dbs, keep = [], []
     for w in ws:
-        # each instance's own launch configuration (the autotuner's choice for
-        # its rows and estimated groups); the persistent launch picks one block
-        # shape for all and keeps each instance's shared-memory strategy
-        aggs.append(vr.GpuHashAggregate(w.columns, w.keys, w.functions, est_groups=w.est_groups,
-                                        max_batch_rows=w.rows, device=device))
         db, t = Cc.to_device(w.batch(), device)
         dbs.append(db)
         keep.append(t)
+
+    def handles():
+        # each instance's own launch configuration: the autotuner's choice for
+        # its (rows, estimated groups) bucket when it has one, else the default
+        return [vr.GpuHashAggregate(w.columns, w.keys, w.functions, est_groups=w.est_groups, max_batch_rows=w.rows,
+                                    device=device) for w in ws]
+
+    # the autotuner, before anything is timed: each estimated-groups bucket's
+    # shared-memory strategy chosen by timing the persistent launch; handles
+    # made afterwards (for both forms below) find its choices
+    aggs = handles()
+    tuner = vr.GpuBatchedAggregate(aggs, dbs, mode=N.VR_BATCHED_PERSISTENT)
+    t0 = time.perf_counter()
+    tuned_ms = tuner.tune(iters=2)
+    tune_s = time.perf_counter() - t0
+    tuner.close()
+    for a in aggs:
+        a.close()
+    aggs = handles()
     stream = torch.cuda.Stream(device=device)
 
     def timed(b, steps, warmup):
@@ -559,6 +573,10 @@ def run_batched(args, rank, world, device, check):
                    "mode": "one persistent launch replayed from a CUDA graph (table clears, aggregate, "
                            "status gather)",
                    "launch": info,
+                   "autotuner": {"tuned_ms": tuned_ms, "seconds": round(tune_s, 1),
+                                 "what": "per estimated-groups bucket: whole shared-memory table, 256/512/1024-slot "
+                                         "hot-key cache or HBM only, by coordinate descent on the launch's time; "
+                                         "both forms below use the tuned choices"},
                    "l2": "inputs larger than L2 (%.2f GB)" % (in_bytes / 1e9)},
         "roofline": {"bound": "hbm", "achieved": alg / (ms_p * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
                      "frac": alg / (ms_p * 1e-3) / 1e9 / peak, "peak_kind": peak_kind, "traffic": None,

@@ -410,6 +410,16 @@ int vr_batched_create(const vr_batched_plan* plan, vr_batched** out);
 /* Resets every instance's table, then aggregates every instance's batch. */
 int vr_batched_run(vr_batched* b, void* stream);
 int vr_batched_get_info(const vr_batched* b, vr_batched_info* info);
+/* The autotuner for the persistent launch: instances grouped by the power of
+ * two of their estimated groups, each group's shared-memory strategy (a
+ * whole table, a 256/512/1,024-slot hot-key cache, or HBM alone) chosen by
+ * coordinate descent on the launch's device time (`iters` timed runs per
+ * candidate, the largest groups by rows first). The chosen strategies stay in
+ * the plan and are recorded in the tuner's table (vr_tune_lookup) for each
+ * instance's (spec, rows, estimated groups) bucket; *best_ms is the launch's
+ * time with them. Runs the launch many times: every instance's table holds
+ * the last run's groups afterwards. */
+int vr_batched_tune(vr_batched* b, int32_t iters, double* best_ms);
 void vr_batched_destroy(vr_batched* b);
 
 /* ---- autotuner (table size, block shape, tier) keyed on rows and

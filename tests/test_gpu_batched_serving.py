@@ -223,3 +223,30 @@ def test_serving_accounts_for_table_growth(cuda):
         assert st.hbm_peak > n * 40, st.hbm_peak
     finally:
         srv.close()
+
+
+def test_batched_autotuner_keeps_results_and_records_its_choices(cuda):
+    """vr_batched_tune picks each estimated-groups bucket's strategy by timing
+    the launch; the results stay the oracle's, and handles created afterwards
+    find the tuner's choice for their (spec, rows, groups) bucket."""
+    import ctypes as C
+
+    ws, aggs, dbs, keep = _instances(24, max_log_rows=15, max_log_card=13)
+    b = vr.GpuBatchedAggregate(aggs, dbs, mode=N.VR_BATCHED_PERSISTENT, use_graph=True)
+    try:
+        ms = b.tune(iters=1)
+        assert ms > 0
+        info = b.info()
+        assert info["whole_tables"] + info["caches"] + info["hbm_only"] == len(ws)
+        b.run()
+        for w, a in zip(ws, aggs):
+            n = a.num_groups()
+            compare(w.spec(), a.output_types, a.emit(), n, *oracle_of(w, [w.batch()]))
+        choice = N.TuneChoice()
+        w = ws[0]
+        assert N.lib().vr_tune_lookup(C.byref(w.spec().spec), w.rows, C.byref(choice)) == 1
+        assert choice.tier in (1, 2)
+    finally:
+        b.close()
+        for a in aggs:
+            a.close()

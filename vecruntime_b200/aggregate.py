@@ -334,6 +334,15 @@ class GpuBatchedAggregate:
         if rc:
             raise N.VrError(rc, "vr_batched_run: " + (self._lib.vr_thread_last_error() or b"").decode())
 
+    def tune(self, iters: int = 2) -> float:
+        """vr_batched_tune: each estimated-groups bucket's shared-memory
+        strategy chosen by measurement; returns the launch's ms with them."""
+        ms = C.c_double()
+        rc = self._lib.vr_batched_tune(self.h, iters, C.byref(ms))
+        if rc:
+            raise N.VrError(rc, "vr_batched_tune: " + (self._lib.vr_thread_last_error() or b"").decode())
+        return ms.value
+
     def info(self) -> dict:
         """The persistent launch's block shape and how many instances use a
         whole shared-memory table, a hot-key cache or HBM alone."""

@@ -10,8 +10,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <cstdlib>
 #include <cstring>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -106,23 +106,26 @@ static int batched_enqueue(vr_batched* b, cudaStream_t st) {
     return VR_OK;
 }
 
-// Tiles a producer takes per grab in the persistent launch: consecutive tiles
-// of one instance, so a small instance is spread over fewer CTAs (each of
-// which flushes its shared-memory table into the instance's HBM table).
-constexpr int kBatchedTileRun = 8;
+// Rows a producer takes per grab in the persistent launch (a run of
+// consecutive tiles of one instance), so a small instance is spread over
+// fewer CTAs, each of which flushes its shared-memory table into the
+// instance's HBM table. Measured on 512 uneven instances (1,024-row tiles):
+// one tile per grab 23.1 ms, 4 tiles 21.4, 8 20.2, 16 19.2, 32 18.7, 128 19.8.
+constexpr int kBatchedRunRows = 32768;
 
 // The persistent launch's block shape (hash tier): one for every instance,
 // since the stage layout and the kernel's thread count are per launch.
-// Measured defaults: two CTAs per SM of 256 consumer threads, 512-row tiles
-// and two stages, which leave a 1,024-slot shared-memory area per CTA for
-// 80-byte slots (a whole table for up to ~700 groups).
+// Measured defaults: two CTAs per SM of 256 consumer threads, 1,024-row
+// tiles and two stages, which leave a 512-slot shared-memory area per CTA
+// for 80-byte slots (a whole table for up to ~350 groups); 512-row tiles
+// (a 1,024-slot area) took 19.6 against 18.7 ms on 512 uneven instances.
 static int batched_shape(vr_batched* b, const vr_tune_choice* shape) {
     vr_agg* h0 = b->inst[0];
     const Program& P = h0->plan.prog;
     const DeviceInfo& di = device_info(b->device);
     const int threads = shape && shape->threads ? shape->threads : 256;
     const int want_ctas = shape && shape->blocks_per_sm ? shape->blocks_per_sm : 2;
-    const int T = shape && shape->tile_rows ? shape->tile_rows : 512;
+    const int T = shape && shape->tile_rows ? shape->tile_rows : 1024;
     if (threads % 32 || threads > kMaxConsumerThreadsJit || T % 128 || T <= 0) {
         set_thread_error("batched shape: threads must be a multiple of 32 up to 512, tiles a multiple of 128");
         return VR_ERR_INVALID;
@@ -139,9 +142,8 @@ static int batched_shape(vr_batched* b, const vr_tune_choice* shape) {
     while (area * 2 * 8 * P.sw <= budget - base) area *= 2;  // power-of-two tables
     LaunchCfg& L = b->cfg;
     L = h0->launch;
-    L.tile_run = kBatchedTileRun;
-    if (const char* e = std::getenv("VRGPU_TILE_RUN")) L.tile_run = std::max(1, std::atoi(e));
     L.tile_rows = T;
+    L.tile_run = std::max(1, kBatchedRunRows / T);
     L.stages = stages;
     L.consumer_threads = threads;
     L.rchunk = 1;
@@ -201,6 +203,8 @@ static void instance_strategy(vr_batched* b, vr_agg* h, BatchDesc& d, int cache_
     d.s_probes = 2;
     b->info.caches++;
 }
+
+static int batched_settle(vr_batched* b);
 
 extern "C" {
 
@@ -400,7 +404,14 @@ int vr_batched_run(vr_batched* b, void* stream) {
         if (rc != VR_OK) return rc;
     }
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return VR_ERR_CUDA;
-    // per-instance bookkeeping: groups, errors, and growth + replay where needed
+    return batched_settle(b);
+}
+
+}  // extern "C"
+
+// Per-instance bookkeeping after a run: groups, errors, and growth + replay
+// where an instance's HBM table was too small.
+static int batched_settle(vr_batched* b) {
     const int n = (int)b->inst.size();
     int status = VR_OK;
     for (int i = 0; i < n; ++i) {
@@ -431,6 +442,151 @@ int vr_batched_run(vr_batched* b, void* stream) {
         }
     }
     return status;
+}
+
+// ---------------------------------------------------------------- autotuner
+// Shared-memory strategies an instance can take in the persistent launch.
+enum Strategy { kWhole = 0, kCache256, kCache512, kCache1024, kHbm, kStrategies };
+
+// Sets instance d's strategy; false when it does not fit the launch's area.
+static bool apply_strategy(const vr_batched* b, const vr_agg* h, BatchDesc& d, int s) {
+    const int64_t area = b->info.smem_slots_max;
+    switch (s) {
+        case kWhole: {
+            const int64_t est = h->spec.est_groups;
+            if (est <= 0) return false;
+            const int64_t need = next_pow2(std::max<int64_t>(64, (est * 10 + 6) / 7));
+            if (need > area) return false;
+            d.smem_slots = (int32_t)need;
+            d.s_probes = 64;
+            return true;
+        }
+        case kCache256:
+        case kCache512:
+        case kCache1024: {
+            const int64_t slots = 256 << (s - kCache256);
+            if (slots > area) return false;
+            d.smem_slots = (int32_t)slots;
+            d.s_probes = 2;
+            return true;
+        }
+        case kHbm:
+            d.smem_slots = 0;
+            d.s_probes = 0;
+            return true;
+    }
+    return false;
+}
+
+static int strategy_of(const BatchDesc& d) {
+    if (d.smem_slots == 0) return kHbm;
+    if (d.s_probes > 2) return kWhole;
+    return d.smem_slots >= 1024 ? kCache1024 : d.smem_slots >= 512 ? kCache512 : kCache256;
+}
+
+// One timed persistent run (device time of the launch, then the bookkeeping).
+static int timed_run(vr_batched* b, cudaStream_t st, cudaEvent_t e0, cudaEvent_t e1, float* ms) {
+    cudaEventRecord(e0, st);
+    int rc = batched_enqueue(b, st);
+    cudaEventRecord(e1, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return VR_ERR_CUDA;
+    if (rc != VR_OK) return rc;
+    cudaEventElapsedTime(ms, e0, e1);
+    return batched_settle(b);
+}
+
+extern "C" {
+
+int vr_batched_tune(vr_batched* b, int32_t iters, double* best_ms) {
+    if (!b || b->mode != VR_BATCHED_PERSISTENT || b->tier == kTierDirect) {
+        set_thread_error("vr_batched_tune: a persistent hash-tier launch only");
+        return VR_ERR_INVALID;
+    }
+    if (iters < 1) iters = 2;
+    cudaSetDevice(b->device);
+    for (vr_agg* h : b->inst) {  // a clear still queued on an instance's own stream goes first
+        if (!h->clear_queued) continue;
+        if (cudaStreamSynchronize(h->stream) != cudaSuccess) return VR_ERR_CUDA;
+        h->clear_queued = false;
+    }
+    cudaStream_t st;
+    cudaEvent_t e0, e1;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return VR_ERR_CUDA;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const int n = (int)b->inst.size();
+    auto upload = [&]() {
+        return cudaMemcpy(b->descs_dev, b->descs.data(), sizeof(BatchDesc) * n, cudaMemcpyHostToDevice) == cudaSuccess;
+    };
+    auto measure = [&](double* out) {
+        double best = 1e30;
+        for (int it = 0; it < iters + 1; ++it) {  // the first run warms up (and grows tables)
+            float ms = 0;
+            int rc = timed_run(b, st, e0, e1, &ms);
+            if (rc != VR_OK) return rc;
+            if (it > 0) best = std::min(best, (double)ms);
+        }
+        *out = best;
+        return (int)VR_OK;
+    };
+    // instances grouped by the power of two of their estimated groups,
+    // the buckets with the most rows tuned first
+    std::map<int, std::vector<int>> buckets;
+    std::map<int, int64_t> bucket_rows;
+    for (int i = 0; i < n; ++i) {
+        const int64_t est = std::max<int64_t>(1, b->inst[i]->spec.est_groups);
+        int k = 0;
+        while ((int64_t(1) << k) < est) ++k;
+        buckets[k].push_back(i);
+        bucket_rows[k] += b->descs[i].num_rows;
+    }
+    std::vector<std::pair<int64_t, int>> order;
+    for (auto& kv : bucket_rows) order.push_back({-kv.second, kv.first});
+    std::sort(order.begin(), order.end());
+    double cur = 0;
+    int rc = measure(&cur);
+    // coordinate descent: each bucket's strategy with the others held fixed
+    for (size_t oi = 0; oi < order.size() && rc == VR_OK; ++oi) {
+        const std::vector<int>& members = buckets[order[oi].second];
+        const int was = strategy_of(b->descs[members[0]]);
+        for (int s = 0; s < kStrategies && rc == VR_OK; ++s) {
+            if (s == was) continue;
+            std::vector<BatchDesc> saved;
+            bool ok = true;
+            for (int i : members) {
+                saved.push_back(b->descs[i]);
+                ok = ok && apply_strategy(b, b->inst[i], b->descs[i], s);
+            }
+            double t = 0;
+            if (ok && upload()) rc = measure(&t);
+            if (!(ok && rc == VR_OK && t < cur * 0.995)) {  // keep a strategy only when it is faster
+                for (size_t j = 0; j < members.size(); ++j) b->descs[members[j]] = saved[j];
+            } else {
+                cur = t;
+            }
+        }
+        if (!upload()) rc = VR_ERR_CUDA;
+    }
+    // the chosen strategies: in the launch's counts, and in the autotuner's
+    // table for each instance's (spec, rows, estimated groups) bucket
+    b->info.whole_tables = b->info.caches = b->info.hbm_only = 0;
+    for (int i = 0; i < n && rc == VR_OK; ++i) {
+        const int s = strategy_of(b->descs[i]);
+        (s == kWhole ? b->info.whole_tables : s == kHbm ? b->info.hbm_only : b->info.caches)++;
+        vr_tune_choice c;
+        std::memset(&c, 0, sizeof(c));
+        c.tier = s == kHbm ? 2 : 1;
+        c.warp_agg = b->descs[i].warp_agg;
+        c.threads = b->cfg.consumer_threads;
+        c.tile_rows = b->cfg.tile_rows;
+        c.smem_slots = s == kWhole ? 0 : b->descs[i].smem_slots;  // 0: the default, a table of every group
+        vr_tune_record(&b->inst[i]->spec, b->descs[i].num_rows, &c, (double)b->total_rows / (cur * 1e-3));
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamDestroy(st);
+    if (best_ms) *best_ms = cur;
+    return rc;
 }
 
 void vr_batched_destroy(vr_batched* b) {

@@ -191,6 +191,7 @@ PROTOTYPES = [
     ("vr_batched_create", C.c_int, [C.POINTER(BatchedPlan), C.POINTER(_P)]),
     ("vr_batched_run", C.c_int, [_P, _P]),
     ("vr_batched_get_info", C.c_int, [_P, C.POINTER(BatchedInfo)]),
+    ("vr_batched_tune", C.c_int, [_P, C.c_int32, C.POINTER(C.c_double)]),
     ("vr_batched_destroy", None, [_P]),
     ("vr_tune_lookup", C.c_int, [C.POINTER(AggSpec), C.c_int64, C.POINTER(TuneChoice)]),
     ("vr_tune_record", C.c_int, [C.POINTER(AggSpec), C.c_int64, C.POINTER(TuneChoice), C.c_double]),
