@@ -301,6 +301,21 @@ class GpuHashAggregate:
             pass
 
 
+def tune_search(columns, keys, functions, device_batch, est_groups: int = 0, max_batch_rows: int = 0,
+                device: int = 0, iters: int = 2):
+    """vr_tune_search: times every candidate launch configuration of the spec
+    on one device-resident batch and records the fastest in the autotuner's
+    table for (spec, rows, estimated groups), where handles created afterwards
+    find it. Returns (choice, rows/s)."""
+    spec = Spec(columns, keys, functions, est_groups, max_batch_rows, device)
+    cb = device_batch.ctypes()
+    best = N.TuneChoice()
+    rps = C.c_double()
+    N.check(N.lib().vr_tune_search(C.byref(spec.spec), C.byref(cb), iters, C.byref(best), C.byref(rps)),
+            "vr_tune_search")
+    return best, rps.value
+
+
 # ------------------------------------------------------------------ batched
 class GpuBatchedAggregate:
     """Many independent aggregates (one Spark task's batch each) run by one

@@ -173,6 +173,9 @@ int vr_tune_search(const vr_agg_spec* spec, const vr_batch* batch, int32_t iters
         add(1, wa, 0, 0, 0, 0);
         for (int tile : {1024, 512, 256})
             for (int slots : {256, 512, 1024}) add(1, wa, 256, tile, slots, 2);
+        // one CTA per SM of 512 threads: room for a 2,048 or 4,096-slot cache
+        // (more of a skewed key's head in shared memory)
+        for (int slots : {2048, 4096}) add(1, wa, 512, 512, slots, 1);
         add(2, wa, 256, 1024, 0, 2);
     }
     double best_v = -1;
