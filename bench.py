@@ -355,8 +355,21 @@ def run_single(args, name, rank, world, device, check):
     w = make_workload(name, args.rows if args.workload == name else None)
     log(f"[rank {rank}] workload {w.name}: {w.rows} rows, est groups {w.est_groups}")
     db, tensors = device_batch(w, device)
+    tuned = None
+    if name in ("highcard", "plain"):
+        # the autotuner, before anything is timed: every candidate shape and
+        # shared-memory size on this batch; the handle below finds the fastest
+        from vecruntime_b200 import aggregate as A
+
+        t0 = time.perf_counter()
+        best, rps = A.tune_search(w.columns, w.keys, w.functions, db, est_groups=w.est_groups, max_batch_rows=w.rows,
+                                  device=device, iters=2)
+        tuned = {"tier": best.tier, "threads": best.threads, "ctas_per_sm": best.blocks_per_sm,
+                 "tile_rows": best.tile_rows, "smem_slots": best.smem_slots, "warp_agg": best.warp_agg,
+                 "seconds": round(time.perf_counter() - t0, 1)}
     agg = vr.GpuHashAggregate(w.columns, w.keys, w.functions, est_groups=w.est_groups, max_batch_rows=w.rows,
                               device=device, flags=N.VR_SPEC_TRACE)
+    launch = agg.stats()
     stream = torch.cuda.ExternalStream(agg.stream(), device=torch.device("cuda", device))
     in_bytes = G.input_bytes(w)
     # before each step's start event, a 1 GiB write on the same stream: it
@@ -408,6 +421,9 @@ def run_single(args, name, rank, world, device, check):
         "dtype": workload_dtype(w),
         "config": {"workload": workload_label(w), "rows_per_gpu": w.rows, "groups": groups,
                    "batch": "one device-resident batch per step",
+                   "launch": {"tier": launch.tier, "threads": launch.threads, "blocks": launch.blocks,
+                              "tile_rows": launch.tile_rows, "smem_bytes": launch.smem_bytes, "jit": launch.jit},
+                   "autotuner": tuned,
                    "l2": "L2 flushed before each step (%d MB written on the stream outside the timed events; "
                          "inputs %.3f GB)" % (FLUSH_BYTES >> 20, in_bytes / 1e9)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
