@@ -460,6 +460,11 @@ int vr_agg_plan(const vr_agg_spec* spec, vr_plan_info* info, vr_column_type* out
  * size; `log` receives the compiler log: the error on failure, ptxas's
  * resource usage (registers, spills, local memory) on success. */
 int vr_jit_compile(const vr_agg_spec* spec, int32_t tier, int64_t* cubin_bytes, char* log, size_t cap);
+/* The same for a given block shape: `threads` consumer threads (plus the
+ * producer warp) and `min_blocks` CTAs per SM, the launch bounds that cap
+ * the kernel's registers. */
+int vr_jit_compile_shape(const vr_agg_spec* spec, int32_t tier, int32_t threads, int32_t min_blocks,
+                         int64_t* cubin_bytes, char* log, size_t cap);
 /* 1 and the recorded choice when the tuner has one for (spec, rows), else 0. */
 int vr_tune_lookup(const vr_agg_spec* spec, int64_t rows, vr_tune_choice* out);
 int vr_tune_record(const vr_agg_spec* spec, int64_t rows, const vr_tune_choice* choice, double rows_per_s);

@@ -1474,7 +1474,12 @@ int vr_hash_rows_noalloc(int32_t num_keys, const vr_column_type* types, const vr
 }
 
 int vr_jit_compile(const vr_agg_spec* spec, int32_t tier, int64_t* cubin_bytes, char* log, size_t cap) {
-    if (!spec) return VR_ERR_INVALID;
+    return vr_jit_compile_shape(spec, tier, 256, 1, cubin_bytes, log, cap);
+}
+
+int vr_jit_compile_shape(const vr_agg_spec* spec, int32_t tier, int32_t threads, int32_t min_blocks,
+                         int64_t* cubin_bytes, char* log, size_t cap) {
+    if (!spec || threads < 32 || threads % 32 || threads > kMaxConsumerThreadsJit || min_blocks < 1) return VR_ERR_INVALID;
     Plan plan;
     int rc = compile_plan(*spec, plan);
     if (rc != VR_OK) {
@@ -1487,6 +1492,8 @@ int vr_jit_compile(const vr_agg_spec* spec, int32_t tier, int64_t* cubin_bytes, 
     shape.kw = plan.prog.kw;
     shape.tier = tier == 0 ? kTierDirect : kTierHash;
     shape.rchunk = tier == 0 ? 4 : 1;
+    shape.threads = threads;
+    shape.min_blocks = min_blocks;
     bool ok = jit_compile_only(plan.prog, shape, &bytes, &err);
     if (log && cap) std::snprintf(log, cap, "%s", err.c_str());
     if (cubin_bytes) *cubin_bytes = (int64_t)bytes;

@@ -200,6 +200,8 @@ PROTOTYPES = [
     ("vr_tune_search", C.c_int, [C.POINTER(AggSpec), C.POINTER(Batch), C.c_int32, C.POINTER(TuneChoice),
                                  C.POINTER(C.c_double)]),
     ("vr_jit_compile", C.c_int, [C.POINTER(AggSpec), C.c_int32, C.POINTER(C.c_int64), C.c_char_p, C.c_size_t]),
+    ("vr_jit_compile_shape", C.c_int, [C.POINTER(AggSpec), C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_int64),
+                                       C.c_char_p, C.c_size_t]),
     ("vr_agg_plan", C.c_int, [C.POINTER(AggSpec), C.POINTER(PlanInfo), C.POINTER(ColumnType), C.c_int32]),
     ("vr_srv_create", C.c_int, [C.POINTER(SrvConfig), C.POINTER(_P)]),
     ("vr_srv_open_query", C.c_int, [_P, C.POINTER(AggSpec), C.POINTER(C.c_int32)]),
