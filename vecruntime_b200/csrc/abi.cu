@@ -495,6 +495,7 @@ int agg_build(const vr_agg_spec* spec, const vr_tune_choice* forced, vr_agg** ou
         // wanted count (registers capped to fit)
         const int want = wanted_ctas(forced);
         shape.min_blocks = ctas_per_sm(di, h->launch.smem_bytes, 0, h->cfg.threads, want);
+        shape.warp_agg = h->cfg.warp_agg;
         h->jit = jit_get(h->plan.prog, shape, h->device, &why);
         if (h->jit) {
             const int bps = ctas_per_sm(di, h->launch.smem_bytes, jit_regs(h->jit), h->cfg.threads, want);

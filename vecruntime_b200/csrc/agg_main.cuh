@@ -647,7 +647,13 @@ VR_DEV void consume_tile(const Program& P, const BatchDesc& D, const LaunchCfg& 
 #endif
     } else {
         const int ss = D.smem_slots < sslots ? D.smem_slots : sslots;
+#if defined(VR_JIT) && !VR_JIT_WARP_AGG
+        // compiled for launches that never pre-aggregate in the warp: the
+        // __match_any_sync and peer-reduction code folds away
+        constexpr bool wa = false;
+#else
         const bool wa = D.warp_agg != 0;
+#endif
         for (int base = 0; base < rows; base += R * NT) {  // uniform trip count: warps stay converged
             int64_t r[R];
             bool live[R];

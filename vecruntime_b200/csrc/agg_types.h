@@ -39,6 +39,6 @@ struct SmemMap {
 
 constexpr int kMaxStages = 4;
 constexpr int kMaxConsumerThreads = 256;     // the prebuilt kernel's launch bounds
-constexpr int kMaxConsumerThreadsJit = 512;  // per-spec kernels take their bounds from the shape
+constexpr int kMaxConsumerThreadsJit = 992;  // per-spec kernels take their bounds from the shape (992 + the producer warp = 1,024)
 
 }  // namespace vr

@@ -160,6 +160,8 @@ static int batched_shape(vr_batched* b, const vr_tune_choice* shape) {
         js.rchunk = 1;
         js.threads = threads;
         js.min_blocks = ctas_per_sm(di, L.smem_bytes, 0, threads, want_ctas);
+        js.warp_agg = 0;  // pre-aggregation compiled in only when an instance uses it
+        for (vr_agg* h : b->inst) js.warp_agg |= h->cfg.warp_agg;
         std::string why;
         b->jit = jit_get(P, js, b->device, &why);
         if (b->jit) regs = jit_regs(b->jit);

@@ -269,6 +269,7 @@ static std::string jit_source(const Program& P, const JitShape& S) {
     std::string src = kPrelude;
     src += "#define VR_JIT_KW " + std::to_string(S.kw) + "\n#define VR_JIT_TIER " + std::to_string(S.tier) + "\n";
     src += "#define VR_JIT_RCHUNK " + std::to_string(S.rchunk) + "\n";
+    src += "#define VR_JIT_WARP_AGG " + std::to_string(S.warp_agg ? 1 : 0) + "\n";
     src += "#define VR_JIT_THREADS " + std::to_string(S.threads) + "\n";
     src += "#define VR_JIT_HW " + std::to_string(P.hw) + "\n#define VR_JIT_AW " + std::to_string(P.aw) + "\n";
     src += "#define VR_JIT_SW " + std::to_string(P.sw) + "\n#define VR_JIT_DSLOTS " +

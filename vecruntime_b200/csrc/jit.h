@@ -23,6 +23,7 @@ struct JitShape {
     int rchunk = 4;
     int threads = 256;
     int min_blocks = 1;
+    int warp_agg = 1;  // 0: no launch of this kernel pre-aggregates in the warp (the code is left out)
 };
 JitKernel* jit_get(const Program& prog, const JitShape& shape, int device, std::string* err);
 int jit_regs(const JitKernel* k);
