@@ -115,15 +115,18 @@ constexpr int kBatchedRunRows = 32768;
 
 // The persistent launch's block shape (hash tier): one for every instance,
 // since the stage layout and the kernel's thread count are per launch.
-// Measured defaults: two CTAs per SM of 256 consumer threads, 1,024-row
-// tiles and two stages, which leave a 512-slot shared-memory area per CTA
-// for 80-byte slots (a whole table for up to ~350 groups); 512-row tiles
-// (a 1,024-slot area) took 19.6 against 18.7 ms on 512 uneven instances.
+// Measured defaults: two CTAs per SM of 512 consumer threads (the per-spec
+// kernel fits them in 64 registers), 1,024-row tiles and two stages, which
+// leave a 512-slot shared-memory area per CTA for 80-byte slots (a whole
+// table for up to ~350 groups). On 512 uneven instances (tiles taken in runs,
+// before / after the autotuner): 2 x 512 threads 13.9 / 12.4 ms, 2 x 384
+// with 768-row tiles 14.9 / 13.6, 1 x 896 with 1,792-row tiles 14.8 / 13.4,
+// 2 x 256 19.1 / 16.8, 2 x 480 with 512-row tiles 22.2 / 20.9.
 static int batched_shape(vr_batched* b, const vr_tune_choice* shape) {
     vr_agg* h0 = b->inst[0];
     const Program& P = h0->plan.prog;
     const DeviceInfo& di = device_info(b->device);
-    const int threads = shape && shape->threads ? shape->threads : 256;
+    const int threads = shape && shape->threads ? shape->threads : 512;
     const int want_ctas = shape && shape->blocks_per_sm ? shape->blocks_per_sm : 2;
     const int T = shape && shape->tile_rows ? shape->tile_rows : 1024;
     if (threads % 32 || threads > kMaxConsumerThreadsJit || T % 128 || T <= 0) {
