@@ -225,23 +225,25 @@ static int choose_config(vr_agg* h, const vr_tune_choice* forced) {
         //    holds all groups is 2x faster than a cache that holds half of them)
         if (use_cache && !(forced && forced->smem_slots)) {
             const int half = di.smem_per_sm / 2 - di.smem_reserved;
+            const bool wide = !(forced && forced->threads) && jit_enabled() && !(fl & VR_SPEC_NO_JIT) &&
+                              !h->prebuilt_only;
             for (int ctas = 2; ctas >= 1 && !done; --ctas) {
                 const int bytes = ctas == 2 ? std::min(half, budget) : budget;
                 for (int T : Ts) {
                     if (forced && forced->tile_rows && T != forced->tile_rows) continue;
+                    if (ctas == 1 && wide && T > 1024 && !(forced && forced->tile_rows)) continue;
                     for (int st = 3; st >= 2 && !done; --st) {
                         if (fit(T, st, bytes) >= need) {
                             c.tile_rows = T;
                             c.stages = st;
                             c.smem_slots = (int)need;
                             c.s_probes = 64;  // at most half full: every key finds its place
-                            // one CTA per SM holds the whole table: give it the
-                            // most consumer warps a per-spec kernel allows
-                            // (measured: 512 threads take 0.20 ms where 256
-                            // take 0.34 ms for 4M rows into 1,000 groups)
-                            if (ctas == 1 && !(forced && forced->threads) && jit_enabled() &&
-                                !(fl & VR_SPEC_NO_JIT) && !h->prebuilt_only)
-                                c.threads = kMaxConsumerThreadsJit;
+                            // one CTA per SM holds the whole table: give it 512
+                            // consumer threads and 1,024-row tiles (measured on
+                            // 40M rows into 1,000 groups: 1.31 ms, where 992
+                            // threads take 1.43 and 768 with 768-row tiles 2.23;
+                            // on 4M rows 512 threads took 0.20 ms, 256 0.34)
+                            if (ctas == 1 && wide) c.threads = kWholeTableThreads;
                             done = true;
                         }
                     }

@@ -39,6 +39,7 @@ struct SmemMap {
 
 constexpr int kMaxStages = 4;
 constexpr int kMaxConsumerThreads = 256;     // the prebuilt kernel's launch bounds
+constexpr int kWholeTableThreads = 512;      // one CTA per SM holding a group table in shared memory
 constexpr int kMaxConsumerThreadsJit = 992;  // per-spec kernels take their bounds from the shape (992 + the producer warp = 1,024)
 
 }  // namespace vr
