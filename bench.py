@@ -65,20 +65,27 @@ FLUSH_BYTES = 1 << 30  # written on the step's stream before each step's start e
 # overstates the lead over the real Vector API path by about that much.
 PORT_NOTE = ("scalar C++ restatement of the reference's general-probe aggregate (GroupKeyTable.lookupOrInsert + "
              "GroupedAccumulators), not its SIMD Vector API path; about half the reference's published per-core rate")
-KERNEL_SOURCES = ("agg_main.cuh", "agg_device.cuh", "agg_types.h", "vr_internal.h", "agg_kernels.cu", "batched.cu")
+# the kernels, the per-spec source generator, the planner (slot layout) and
+# the launch-shape choice: what a DRAM byte count depends on
+KERNEL_SOURCES = ("agg_main.cuh", "agg_device.cuh", "agg_types.h", "vr_internal.h", "agg_kernels.cu", "batched.cu",
+                  "jit.cpp", "plan.cpp", "abi.cu")
 
-# DRAM bytes (read + write) per aggregate launch from `ncu --metrics
-# dram__bytes_read.sum,dram__bytes_write.sum` captures, each with the sha1
-# prefix of the kernel sources it was taken on (KERNEL_SOURCES): a figure
-# whose sources changed since is reported as null, not carried over. The
-# decimal report's traffic is its input plus a fixed flush, so a capture at
-# `rows` scales with rows; a hash table's traffic follows its group count, so
-# those captures hold only at their own row count.
+# DRAM bytes (read + write) per aggregate launch, dram__bytes_read.sum +
+# dram__bytes_write.sum of one ncu capture, with the sha1 prefix of the
+# sources it was taken on (KERNEL_SOURCES): a figure whose sources changed
+# since is reported as null, not carried over. Scaling to the timed launch:
+#   "rows"   -- traffic is the input plus a fixed part: scaled by rows;
+#   "approx" -- a hash table's slot traffic per row grows slowly with the
+#               group count; scaled by rows from the smaller capture, so a
+#               little low (earlier sources: 93 B/row at 8M high-cardinality
+#               rows, 103 B/row at 100M);
+#   "exact"  -- captured at the timed size.
 TRAFFIC = {
-    # name: (kernel sources sha1 prefix, rows captured, GB per launch, scales with rows)
-    "decimal": ("", 8_000_000, (320.097792e6 + 4.176128e6) / 1e9, True),
-    "plain": ("", 1 << 20, (25.473792e6 + 6.912e3) / 1e9, False),
-    "highcard": ("", 100_000_000, (7.72e9 + 2.57e9) / 1e9, False),
+    # name: (kernel sources sha1 prefix, rows captured, GB per launch, scaling)
+    "decimal": ("92235e5bbdd0", 8_000_000, (320.077568e6 + 7.250432e6) / 1e9, "rows"),
+    "plain": ("92235e5bbdd0", 1 << 20, (25.449984e6 + 768) / 1e9, "exact"),
+    "highcard": ("92235e5bbdd0", 8_000_000, (555.012608e6 + 186.404096e6) / 1e9, "approx"),
+    "batched": ("92235e5bbdd0", 30_418_299, (1.313819e9 + 464.094464e6) / 1e9, "approx"),
 }
 
 
@@ -100,14 +107,17 @@ def launch_traffic(name, rows):
     t = TRAFFIC.get(name)
     if t is None:
         return None, "no ncu capture of this workload"
-    sha, at, gb, scales = t
+    sha, at, gb, scaling = t
     now = kernel_sha()
     if sha != now:
         return None, f"no ncu capture of the current kernel sources ({now}); the last one was taken on {sha or 'older sources'}"
-    if scales:
-        return gb * rows / at, f"GB per launch ({src}, {at}-row capture on kernel sources {sha}, scaled by rows)"
     if rows == at:
         return gb, f"GB per launch ({src}, capture of this workload on kernel sources {sha})"
+    if scaling == "rows":
+        return gb * rows / at, f"GB per launch ({src}, {at}-row capture on kernel sources {sha}, scaled by rows)"
+    if scaling == "approx":
+        return gb * rows / at, (f"GB per launch ({src}, {at}-row capture on kernel sources {sha}, scaled by rows; "
+                                "table traffic per row grows slowly with groups, so a little low)")
     return None, "no capture at this row count (table traffic follows the group count, not the rows)"
 
 
@@ -356,7 +366,15 @@ def run_single(args, name, rank, world, device, check):
     log(f"[rank {rank}] workload {w.name}: {w.rows} rows, est groups {w.est_groups}")
     db, tensors = device_batch(w, device)
     tuned = None
-    if name in ("highcard", "plain"):
+    forced = None
+    if args.shape:
+        # a fixed launch shape (tier, threads, CTAs per SM, tile rows, shared
+        # slots, warp pre-aggregation), e.g. the one the autotuner picked at
+        # full size, for a profile of a smaller case
+        t, th, ctas, tile, slots, wa = (int(x) for x in args.shape.split(","))
+        forced = N.TuneChoice(t, wa, th, ctas, tile, slots, 0)
+        tuned = {"forced": args.shape}
+    elif name in ("highcard", "plain") and not args.no_tune:
         # the autotuner, before anything is timed: every candidate shape and
         # shared-memory size on this batch; the handle below finds the fastest
         from vecruntime_b200 import aggregate as A
@@ -368,7 +386,7 @@ def run_single(args, name, rank, world, device, check):
                  "tile_rows": best.tile_rows, "smem_slots": best.smem_slots, "warp_agg": best.warp_agg,
                  "seconds": round(time.perf_counter() - t0, 1)}
     agg = vr.GpuHashAggregate(w.columns, w.keys, w.functions, est_groups=w.est_groups, max_batch_rows=w.rows,
-                              device=device, flags=N.VR_SPEC_TRACE)
+                              device=device, flags=N.VR_SPEC_TRACE, tune=forced)
     launch = agg.stats()
     stream = torch.cuda.ExternalStream(agg.stream(), device=torch.device("cuda", device))
     in_bytes = G.input_bytes(w)
@@ -538,14 +556,16 @@ def run_batched(args, rank, world, device, check):
     # shared-memory strategy chosen by timing the persistent launch; handles
     # made afterwards (for both forms below) find its choices
     aggs = handles()
-    tuner = vr.GpuBatchedAggregate(aggs, dbs, mode=N.VR_BATCHED_PERSISTENT)
-    t0 = time.perf_counter()
-    tuned_ms = tuner.tune(iters=2)
-    tune_s = time.perf_counter() - t0
-    tuner.close()
-    for a in aggs:
-        a.close()
-    aggs = handles()
+    tuned_ms, tune_s = None, 0.0
+    if not args.no_tune:
+        tuner = vr.GpuBatchedAggregate(aggs, dbs, mode=N.VR_BATCHED_PERSISTENT)
+        t0 = time.perf_counter()
+        tuned_ms = tuner.tune(iters=2)
+        tune_s = time.perf_counter() - t0
+        tuner.close()
+        for a in aggs:
+            a.close()
+        aggs = handles()
     stream = torch.cuda.Stream(device=device)
 
     def timed(b, steps, warmup):
@@ -580,6 +600,7 @@ def run_batched(args, rank, world, device, check):
     peak, peak_kind = measured_peaks()
     out_bytes = sum(groups) * output_row_bytes(out_types)
     alg = in_bytes + out_bytes
+    traffic, traffic_unit = launch_traffic("batched", rows)
     rec = {
         "value": value, "unit": "rows/s", "ms_per_step": ms_p, "steps": args.steps, "warmup": args.warmup,
         "dtype": "int64/f64",
@@ -589,14 +610,14 @@ def run_batched(args, rank, world, device, check):
                    "mode": "one persistent launch replayed from a CUDA graph (table clears, aggregate, "
                            "status gather)",
                    "launch": info,
-                   "autotuner": {"tuned_ms": tuned_ms, "seconds": round(tune_s, 1),
+                   "autotuner": None if args.no_tune else {"tuned_ms": tuned_ms, "seconds": round(tune_s, 1),
                                  "what": "per estimated-groups bucket: whole shared-memory table, 256/512/1024-slot "
                                          "hot-key cache or HBM only, by coordinate descent on the launch's time; "
                                          "both forms below use the tuned choices"},
                    "l2": "inputs larger than L2 (%.2f GB)" % (in_bytes / 1e9)},
         "roofline": {"bound": "hbm", "achieved": alg / (ms_p * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
-                     "frac": alg / (ms_p * 1e-3) / 1e9 / peak, "peak_kind": peak_kind, "traffic": None,
-                     "traffic_unit": "no ncu capture of the batched launch",
+                     "frac": alg / (ms_p * 1e-3) / 1e9 / peak, "peak_kind": peak_kind, "traffic": traffic,
+                     "traffic_unit": traffic_unit,
                      "algorithmic_bytes_per_launch": alg,
                      "kernel_ms": ms_p, "kernel_ms_is": "the whole graph (table clears + aggregate + status gather)"},
         "one_launch_per_instance": {"value": value_l, "unit": "rows/s", "ms_per_step": ms_l,
@@ -890,6 +911,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-parity", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (default launch shapes)")
+    ap.add_argument("--shape", default=None,
+                    help="decimal/plain/highcard: a fixed launch shape tier,threads,ctas,tile,slots,warp_agg")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

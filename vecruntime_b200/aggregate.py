@@ -321,9 +321,11 @@ class GpuBatchedAggregate:
     """Many independent aggregates (one Spark task's batch each) run by one
     persistent launch (mode VR_BATCHED_PERSISTENT, optionally replayed from a
     CUDA graph) or by one launch per instance (VR_BATCHED_PLAIN). The
-    instances must share one spec shape and one launch configuration: create
-    them with the same `tune` choice. No reference counterpart: the reference
-    runs one task per thread (VectorHashAggregateExec.scala:248-302)."""
+    instances share one spec (the same functions over the same column types)
+    and one tier; each keeps its own table and shared-memory strategy (whole
+    table, hot-key cache or HBM only), which `tune` chooses per estimated-groups
+    bucket. No reference counterpart: the reference runs one task per thread
+    (VectorHashAggregateExec.scala:248-302)."""
 
     def __init__(self, instances: Sequence["GpuHashAggregate"], device_batches: Sequence, mode: int = 0,
                  use_graph: bool = False, shape: Optional[N.TuneChoice] = None):
