@@ -518,6 +518,63 @@ int vr_srv_get_stats(vr_srv* s, vr_srv_stats* st);
 int vr_srv_drain(vr_srv* s);
 void vr_srv_destroy(vr_srv* s);
 
+/* ---- Parquet data pages -> Arrow columns on the device -------------------
+ * The scan that feeds the aggregate: a column chunk's data pages, already
+ * decompressed into device memory, decoded into one Arrow column without a
+ * trip through host memory. Replaces ParquetPageDecoder.decode
+ * (parquet/src/main/java/io/vecruntime/parquet/codec/ParquetPageDecoder.java:214-266)
+ * with RleBitPackingReader (RleBitPackingReader.java:117-392) for the
+ * definition levels and the dictionary ids, for flat columns (no repetition
+ * levels). An RLE_DICTIONARY page decodes to its dictionary ids (int32), not
+ * to resolved values: the column goes to the aggregate as VR_DICT32 with the
+ * chunk's dictionary attached as a batch dictionary (VR_COL_BATCH_DICTIONARY;
+ * vr_pq_plain_dictionary decodes a BYTE_ARRAY dictionary page into one), and
+ * the aggregate maps each dictionary onto its table's once per batch. A
+ * PLAIN page of a fixed-width type decodes to its values, a null slot
+ * holding 0 (the reference leaves it unspecified). */
+enum vr_pq_encoding { VR_PQ_PLAIN = 0, VR_PQ_RLE_DICTIONARY = 1 };
+
+typedef struct vr_pq_page {
+    const uint8_t* data;    /* device: the decompressed page. v1: [int32 LE byte length of
+                               the levels][levels][values]; v2: [levels][values]; without
+                               definition levels (max_def_level 0) only the values. RLE_DICTIONARY
+                               values: one byte of id bit width, then the id stream */
+    int64_t length;         /* bytes of the page */
+    int32_t num_values;     /* slots in the page (one definition level each) */
+    int32_t max_def_level;  /* a slot is present when its level equals this; 0: all present */
+    int32_t v2;             /* data page v2: the levels' byte length is levels_length */
+    int32_t levels_length;  /* v2 only */
+    int32_t encoding;       /* enum vr_pq_encoding; every page of one call has the same */
+    int32_t value_bytes;    /* PLAIN: 4 (INT32, FLOAT) or 8 (INT64, DOUBLE); RLE_DICTIONARY: 4 */
+} vr_pq_page;
+
+typedef struct vr_pq_decoder vr_pq_decoder;
+/* A decoder on `device` for calls of up to `max_values` slots and
+ * `max_bytes` page bytes in total (it sizes its device scratch for them). */
+int vr_pq_create(int32_t device, int64_t max_values, int64_t max_bytes, vr_pq_decoder** out);
+/* Decodes `num_pages` pages of one column chunk, in order, into one column
+ * of the pages' slots in order: out_data (device; value_bytes per slot) and
+ * out_validity (device, LSB-first bitmap, ceil(slots / 8) bytes; may be
+ * NULL when no page has definition levels). Asynchronous on `stream` (a
+ * cudaStream_t; NULL = the decoder's own). `pages` is read before the call
+ * returns. A malformed page (a run header or payload past its stream, an
+ * id stream with fewer ids than present slots, a bit width above 32) is
+ * reported by vr_pq_sync. */
+int vr_pq_decode(vr_pq_decoder* d, int32_t num_pages, const vr_pq_page* pages, void* out_data,
+                 uint8_t* out_validity, void* stream);
+/* Waits for the last decode; `present` (may be NULL) receives its count of
+ * present slots. VR_ERR_INVALID for a malformed page, the page and the
+ * reason in vr_thread_last_error (as for every vr_pq_* error). */
+int vr_pq_sync(vr_pq_decoder* d, int64_t* present);
+void vr_pq_destroy(vr_pq_decoder* d);
+/* Host: a PLAIN-encoded BYTE_ARRAY dictionary page (num_values entries of an
+ * int32 LE length and the bytes) into vr_dictionary buffers: offsets
+ * (num_values + 1 int32) and data (*data_bytes bytes). With data == NULL it
+ * only sets *data_bytes. Replaces ParquetPageDecoder.decodeDictionary
+ * (ParquetPageDecoder.java:440-513) for BYTE_ARRAY. */
+int vr_pq_plain_dictionary(const uint8_t* page, int64_t length, int32_t num_values, int32_t* offsets,
+                           uint8_t* data, int64_t* data_bytes);
+
 #ifdef __cplusplus
 }
 #endif

@@ -11,6 +11,9 @@
  *   GroupedAccumulators               kernels/src/main/java/io/vecruntime/kernels/GroupedAccumulators.java
  *   AggKernels / CompareOp NaN rules  AggKernels.java:40-41, 446-522; CompareOp.java:68-81
  *   Spark buffer rules                spark/src/main/scala/io/vecruntime/spark/agg/VectorAggregates.scala
+ *   Parquet page decoding (pq_oracle.cpp)
+ *                                     parquet/src/main/java/io/vecruntime/parquet/codec/RleBitPackingReader.java,
+ *                                     ParquetPageDecoder.java:214-311, 415-497
  * It shares only the ABI structs (vrgpu.h) with the product; its table,
  * hashing and accumulators are its own code.
  */
@@ -62,6 +65,16 @@ int orc_agg_key_dictionary(const orc_agg* a, int32_t key, int32_t* size, int32_t
 /* The same partitioned run folded into `dst` (the full-size parity check:
  * every group of the batch, ready for orc_agg_emit). */
 int orc_agg_update_threads(orc_agg* dst, const vr_batch* batch, int32_t threads, int64_t chunk_rows);
+
+/* Parquet pages (pq_oracle.cpp): RleBitPackingReader.readInts of n values
+ * from a fresh reader, and ParquetPageDecoder.decode of one flat page into
+ * ids / values and validity as vr_pq_decode writes them. */
+int orc_rle_decode(const uint8_t* buf, int64_t len, int32_t bit_width, int64_t n, uint32_t* out);
+int orc_pq_decode_page(const uint8_t* page, const vr_pq_page* desc, void* out_data, uint8_t* out_validity,
+                       int64_t* present_count);
+int orc_pq_plain_dictionary(const uint8_t* page, int64_t length, int32_t num_values, int32_t* offsets,
+                            uint8_t* data, int64_t* data_bytes);
+const char* orc_pq_last_error(void);
 
 #ifdef __cplusplus
 }

@@ -51,6 +51,10 @@ def lib():
         L.orc_agg_update_threads.argtypes = [P, C.POINTER(N.Batch), C.c_int32, C.c_int64]
         L.orc_agg_run_threads.argtypes = [C.POINTER(N.AggSpec), C.POINTER(N.Batch), C.c_int32, C.c_int64,
                                           C.POINTER(C.c_double), C.POINTER(C.c_int64)]
+        L.orc_rle_decode.argtypes = [P, C.c_int64, C.c_int32, C.c_int64, P]
+        L.orc_pq_decode_page.argtypes = [P, C.POINTER(N.PqPage), P, P, C.POINTER(C.c_int64)]
+        L.orc_pq_plain_dictionary.argtypes = [P, C.c_int64, C.c_int32, P, P, C.POINTER(C.c_int64)]
+        L.orc_pq_last_error.restype = C.c_char_p
         _lib = L
     return _lib
 
@@ -154,3 +158,51 @@ def run_threads(spec, batch, threads: int, chunk_rows: int = 4096):
     if rc:
         raise OracleError(rc, lib().orc_last_error().decode())
     return secs.value, groups.value
+
+
+# ------------------------------------------------------------------ Parquet pages
+def _buf(data: bytes):
+    """`data` with 8 bytes of slack after it (the reference tests' segments
+    carry the same), as a ctypes buffer."""
+    return C.create_string_buffer(bytes(data) + b"\0" * 8, len(data) + 8)
+
+
+def rle_decode(data: bytes, width: int, n: int) -> np.ndarray:
+    """RleBitPackingReader.readInts of n values (uint32)."""
+    out = np.zeros(max(n, 1), np.uint32)
+    b = _buf(data)
+    rc = lib().orc_rle_decode(b, len(data), width, n, out.ctypes.data)
+    if rc:
+        raise OracleError(rc, lib().orc_pq_last_error().decode())
+    return out[:n]
+
+
+def pq_decode_page(data: bytes, **fields):
+    """ParquetPageDecoder.decode of one flat page: (slot bytes, validity
+    bitmap bytes, present count); ids for a dictionary page, 0 at a null."""
+    page = N.PqPage(None, len(data), **fields)
+    vb = 4 if fields.get("encoding") == N.VR_PQ_RLE_DICTIONARY else fields["value_bytes"]
+    n = fields["num_values"]
+    out = np.zeros(max(n, 1) * vb, np.uint8)
+    valid = np.zeros(max(1, (n + 7) // 8), np.uint8)
+    present = C.c_int64()
+    b = _buf(data)
+    rc = lib().orc_pq_decode_page(b, C.byref(page), out.ctypes.data, valid.ctypes.data, C.byref(present))
+    if rc:
+        raise OracleError(rc, lib().orc_pq_last_error().decode())
+    return out[:n * vb], valid[:(n + 7) // 8], present.value
+
+
+def pq_plain_dictionary(data: bytes, n: int):
+    """ParquetPageDecoder.decodeDictionary (BYTE_ARRAY): (offsets, bytes)."""
+    total = C.c_int64()
+    b = _buf(data)
+    rc = lib().orc_pq_plain_dictionary(b, len(data), n, None, None, C.byref(total))
+    if rc:
+        raise OracleError(rc, lib().orc_pq_last_error().decode())
+    offs = np.zeros(n + 1, np.int32)
+    out = np.zeros(max(1, total.value), np.uint8)
+    rc = lib().orc_pq_plain_dictionary(b, len(data), n, offs.ctypes.data, out.ctypes.data, C.byref(total))
+    if rc:
+        raise OracleError(rc, lib().orc_pq_last_error().decode())
+    return offs, out[:total.value]

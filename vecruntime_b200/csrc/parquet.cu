@@ -1,0 +1,615 @@
+// Parquet data pages -> Arrow columns on the device: the scan side of the
+// aggregate (vr_pq_* in vrgpu.h). A column chunk's decompressed pages sit in
+// device memory; one call decodes a run of them into one column:
+//
+//   1. k_pq_walk    one warp per (page, stream): the RLE / bit-packed hybrid
+//                   run headers of the definition levels and of the
+//                   dictionary ids, walked in order (each header's position
+//                   depends on the previous run), into a run table;
+//   2. k_pq_expand  one warp per run, lanes over its values: levels become
+//                   present flags (level == max_def_level), ids go to a
+//                   compact per-page array (or straight to the output when a
+//                   page has no levels);
+//   3. a CUB exclusive scan of the present flags: each slot's rank among the
+//                   present slots of the call;
+//   4. k_pq_gather  one thread per slot: the slot's id or PLAIN value (the
+//                   rank-th present value of its page), 0 at a null slot, and
+//                   the validity bitmap one warp ballot per 32 slots.
+//
+// Reference: ParquetPageDecoder.decode (parquet/src/main/java/io/vecruntime/
+// parquet/codec/ParquetPageDecoder.java:214-311) and RleBitPackingReader
+// (RleBitPackingReader.java:117-392), for flat columns. Every read stays
+// inside its page: headers and payloads are bounds-checked against their
+// stream before they are read, and a malformed stream stops its walk with
+// a reason the host reports.
+#include <cuda_runtime.h>
+
+#include <cub/device/device_scan.cuh>
+#include <thrust/iterator/transform_iterator.h>
+
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "runtime.h"
+
+namespace vr {
+namespace {
+
+// One run of a stream: `begin` = index of its first value in the stream,
+// bit 31 set for a bit-packed run; `word` = the repeated value of an RLE run
+// or the page byte offset of a bit-packed run's first group. A run's count
+// is the next entry's begin minus its own (the walk writes a terminator).
+struct RunEntry {
+    uint32_t begin;
+    uint32_t word;
+};
+constexpr uint32_t kPacked = 0x80000000u;
+// A run longer than this is recorded as several entries (a bit-packed one at
+// group boundaries: kChunk is a multiple of 8), so one warp expands at most
+// kChunk values and a page of one long RLE run still spreads over warps.
+constexpr int64_t kChunk = 4096;
+
+enum PqReason : int32_t {
+    PQ_OK = 0,
+    PQ_LEVELS_SHORT = 1,    // the level stream ends or is malformed before num_values levels
+    PQ_IDS_SHORT = 2,       // the id stream ends or is malformed before the present slots' ids
+    PQ_PLAIN_SHORT = 3,     // PLAIN values past the end of the page
+    PQ_BAD_WIDTH = 4,       // an id bit width above 32
+    PQ_LEVELS_PAST_END = 5, // the levels' byte length runs past the page
+    PQ_TOO_MANY_RUNS = 6,   // more runs than the run table's share for the stream
+};
+
+// A page as the kernels see it (host-filled; the walk fills the rest).
+struct PqDev {
+    const uint8_t* data;
+    int64_t length;
+    int64_t slot_base;       // first slot of the page in the call's column
+    int64_t run_base[2];     // first run-table entry of the level / value stream
+    int32_t run_cap[2];      // entries the stream may use (terminator included)
+    int32_t num_values;
+    int32_t max_def;
+    int32_t v2;
+    int32_t levels_length;
+    int32_t encoding;
+    int32_t value_bytes;
+    // written by k_pq_walk
+    int64_t values_start;    // first byte of the values region
+    int32_t runs[2];         // runs recorded per stream
+    int32_t decoded[2];      // values the runs cover (at most num_values)
+    int32_t width[2];        // bit width per stream
+    int32_t pad_;
+};
+
+// status[0] reason, [1] page (first error wins); [2..3] present count (u64)
+__device__ void pq_fail(int32_t* status, int reason, int page) {
+    if (atomicCAS(status, 0, reason) == 0) atomicExch(status + 1, page);
+}
+
+__device__ uint32_t ld_le(const uint8_t* p, int n) {
+    uint32_t v = 0;
+    for (int i = 0; i < n; ++i) v |= (uint32_t)__ldg(p + i) << (8 * i);
+    return v;
+}
+
+__device__ int width_of(int max_value) { return max_value ? 32 - __clz(max_value) : 0; }
+
+// Walks [pos, end) of page `d`'s bytes (lane 0 of the warp): run headers in
+// order, each bounds-checked with its payload, until `need` values are
+// covered or the stream stops. Returns the values covered.
+__device__ int64_t walk_stream(const uint8_t* base, int64_t pos, int64_t end, int w, int64_t need,
+                               RunEntry* runs, int32_t cap, int32_t& nruns) {
+    int32_t k = 0;
+    int64_t got = 0;
+    if (w == 0) {  // every value is 0 and no byte is read
+        if (need > 0 && cap >= 2) {
+            runs[0] = RunEntry{0u, 0u};
+            k = 1;
+            got = need;
+        }
+    } else {
+        const int vbytes = (w + 7) >> 3;
+        while (got < need && pos < end) {
+            uint32_t h = 0;
+            bool ok = false;
+            for (int shift = 0; shift <= 28 && pos < end; shift += 7) {
+                const uint8_t b = __ldg(base + pos++);
+                h |= (uint32_t)(b & 0x7F) << shift;
+                if (!(b & 0x80)) {
+                    ok = true;
+                    break;
+                }
+            }
+            if (!ok) break;  // a header cut by the end of the stream
+            const int64_t count = h >> 1;
+            const bool packed = h & 1;
+            int64_t nvals;
+            uint32_t word;
+            if (packed) {
+                const int64_t bytes = count * w;
+                if (pos + bytes > end) break;  // a bit-packed run past the end
+                nvals = count * 8;
+                word = (uint32_t)pos;
+                pos += bytes;
+            } else {
+                if (pos + vbytes > end) break;  // an RLE value past the end
+                word = ld_le(base + pos, vbytes);
+                pos += vbytes;
+                nvals = count;
+            }
+            // entries of at most kChunk values, none past the values needed
+            for (int64_t off = 0; off < nvals && got < need; off += kChunk) {
+                if (k + 1 >= cap) {
+                    got = -1;  // no room (a malformed stream: valid ones fit by construction)
+                    break;
+                }
+                runs[k++] = RunEntry{(uint32_t)got | (packed ? kPacked : 0u),
+                                     packed ? word + (uint32_t)(off / 8 * w) : word};
+                got += nvals - off < kChunk ? nvals - off : kChunk;
+            }
+            if (got < 0) break;
+        }
+    }
+    if (got < 0) {
+        nruns = 0;
+        return -1;
+    }
+    const int64_t cover = got < need ? got : need;
+    runs[k].begin = (uint32_t)cover;  // terminator: the end of the last run
+    nruns = k;
+    return cover;
+}
+
+__global__ void k_pq_walk(PqDev* __restrict__ pages, RunEntry* __restrict__ runs, int32_t* __restrict__ status) {
+    const int p = blockIdx.x;
+    const int s = threadIdx.x >> 5;  // 0: definition levels, 1: values
+    if ((threadIdx.x & 31) != 0) return;
+    PqDev& d = pages[p];
+    const uint8_t* base = d.data;
+    int64_t lstart = 0, llen = 0;
+    if (d.max_def > 0) {
+        if (d.v2) {
+            llen = d.levels_length;
+        } else {
+            if (d.length < 4) {
+                if (s == 0) pq_fail(status, PQ_LEVELS_PAST_END, p);
+                return;
+            }
+            lstart = 4;
+            llen = (int32_t)ld_le(base, 4);
+        }
+        if (llen < 0 || lstart + llen > d.length) {
+            if (s == 0) pq_fail(status, PQ_LEVELS_PAST_END, p);
+            return;
+        }
+    }
+    const int64_t vstart = lstart + llen;
+    if (s == 0) {
+        d.values_start = vstart;
+        if (d.max_def == 0) {
+            d.runs[0] = 0;
+            d.decoded[0] = d.num_values;
+            return;
+        }
+        const int w = width_of(d.max_def);
+        d.width[0] = w;
+        int32_t nr = 0;
+        const int64_t got = walk_stream(base, lstart, lstart + llen, w, d.num_values, runs + d.run_base[0],
+                                        d.run_cap[0], nr);
+        d.runs[0] = nr;
+        d.decoded[0] = got < 0 ? 0 : (int32_t)got;
+        if (got < 0) pq_fail(status, PQ_TOO_MANY_RUNS, p);
+        else if (got < d.num_values) pq_fail(status, PQ_LEVELS_SHORT, p);
+        return;
+    }
+    if (d.encoding != VR_PQ_RLE_DICTIONARY) {  // PLAIN: the values region is the values
+        d.runs[1] = 0;
+        const int64_t avail = (d.length - vstart) / d.value_bytes;
+        d.decoded[1] = (int32_t)(avail < d.num_values ? (avail < 0 ? 0 : avail) : d.num_values);
+        return;
+    }
+    if (vstart >= d.length) {  // no id bit width byte
+        d.runs[1] = 0;
+        d.decoded[1] = 0;
+        return;
+    }
+    const int w = __ldg(base + vstart);
+    d.width[1] = w;
+    if (w > 32) {
+        d.runs[1] = 0;
+        d.decoded[1] = 0;
+        pq_fail(status, PQ_BAD_WIDTH, p);
+        return;
+    }
+    int32_t nr = 0;
+    const int64_t got = walk_stream(base, vstart + 1, d.length, w, d.num_values, runs + d.run_base[1], d.run_cap[1], nr);
+    d.runs[1] = nr;
+    d.decoded[1] = got < 0 ? 0 : (int32_t)got;
+    if (got < 0) pq_fail(status, PQ_TOO_MANY_RUNS, p);
+}
+
+// Value i of a bit-packed run whose payload starts at `payload`: its bits
+// lie in bytes [payload + i*w/8, payload + ceil((i+1)*w/8)), all inside the
+// run's checked payload.
+__device__ uint32_t packed_value(const uint8_t* payload, int64_t i, int w) {
+    const int64_t bit = i * w;
+    const uint8_t* b = payload + (bit >> 3);
+    const int sh = (int)(bit & 7);
+    const int nbytes = (sh + w + 7) >> 3;
+    uint64_t v = 0;
+    for (int j = 0; j < nbytes; ++j) v |= (uint64_t)__ldg(b + j) << (8 * j);
+    v >>= sh;
+    return (uint32_t)(w == 32 ? v : (v & ((1ull << w) - 1)));
+}
+
+// One warp per run, lanes over its values. present: a byte per slot;
+// compact: a page's ids at slot_base + value index; out: the output column
+// (ids of pages without levels go there directly).
+__global__ void k_pq_expand(const PqDev* __restrict__ pages, int num_pages, const RunEntry* __restrict__ runs,
+                            uint8_t* __restrict__ present, int32_t* __restrict__ compact, int32_t* __restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int p = 0; p < num_pages; ++p) {
+        const PqDev& d = pages[p];
+        for (int s = 0; s < 2; ++s) {
+            const int nr = d.runs[s];
+            if (s == 1 && d.encoding != VR_PQ_RLE_DICTIONARY) continue;
+            const RunEntry* R = runs + d.run_base[s];
+            const int w = d.width[s];
+            for (int64_t k = warp; k < nr; k += nwarps) {
+                const RunEntry e = R[k];
+                const int64_t b0 = e.begin & ~kPacked;
+                const int64_t cnt = (int64_t)(R[k + 1].begin & ~kPacked) - b0;
+                const bool packed = (e.begin & kPacked) != 0;
+                const uint8_t* payload = d.data + e.word;
+                for (int64_t i = lane; i < cnt; i += 32) {
+                    const uint32_t v = packed ? packed_value(payload, i, w) : e.word;
+                    const int64_t slot = d.slot_base + b0 + i;
+                    if (s == 0)
+                        present[slot] = v == (uint32_t)d.max_def;
+                    else if (d.max_def > 0)
+                        compact[slot] = (int32_t)v;
+                    else
+                        out[slot] = (int32_t)v;
+                }
+            }
+        }
+    }
+}
+
+struct ToInt {
+    __host__ __device__ int32_t operator()(uint8_t x) const { return x; }
+};
+
+// The page of slot i: the last page whose slot_base <= i.
+__device__ int page_of(const PqDev* pages, int num_pages, int64_t i) {
+    int lo = 0, hi = num_pages - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (pages[mid].slot_base <= i) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// One thread per slot (warps on 32-slot boundaries, so each ballot is one
+// whole validity word).
+__global__ void k_pq_gather(const PqDev* __restrict__ pages, int num_pages, int64_t n,
+                            const uint8_t* __restrict__ present, const int32_t* __restrict__ rank,
+                            const int32_t* __restrict__ compact, uint8_t* __restrict__ out, int vb,
+                            uint8_t* __restrict__ validity, int32_t* __restrict__ status) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    bool valid = false;
+    if (i < n) {
+        const int p = page_of(pages, num_pages, i);
+        const PqDev& d = pages[p];
+        const bool levels = d.max_def > 0;
+        valid = levels ? present[i] != 0 : true;
+        const int64_t r = levels ? (int64_t)rank[i] - rank[d.slot_base] : i - d.slot_base;
+        uint8_t* dst = out + i * vb;
+        if (!valid) {
+            for (int j = 0; j < vb; ++j) dst[j] = 0;
+        } else if (r >= d.decoded[1]) {
+            for (int j = 0; j < vb; ++j) dst[j] = 0;
+            pq_fail(status, d.encoding == VR_PQ_RLE_DICTIONARY ? PQ_IDS_SHORT : PQ_PLAIN_SHORT, p);
+        } else if (d.encoding == VR_PQ_RLE_DICTIONARY) {
+            if (levels) reinterpret_cast<int32_t*>(out)[i] = compact[d.slot_base + r];
+        } else {
+            const uint8_t* src = d.data + d.values_start + r * vb;
+            for (int j = 0; j < vb; ++j) dst[j] = __ldg(src + j);
+        }
+    }
+    const uint32_t word = __ballot_sync(0xffffffffu, valid);
+    const int64_t base = i - lane;
+    if (lane == 0 && base < n) {
+        if (validity) {
+            const int64_t nbytes = (n + 7) >> 3;
+            for (int j = 0; j < 4 && (base >> 3) + j < nbytes; ++j) validity[(base >> 3) + j] = (uint8_t)(word >> (8 * j));
+        }
+        atomicAdd(reinterpret_cast<unsigned long long*>(status + 2), (unsigned long long)__popc(word));
+    }
+}
+
+const char* reason_text(int r) {
+    switch (r) {
+        case PQ_LEVELS_SHORT: return "the definition-level stream ends or is malformed before the page's slots";
+        case PQ_IDS_SHORT: return "the dictionary-id stream ends or is malformed before the page's present slots";
+        case PQ_PLAIN_SHORT: return "PLAIN values past the end of the page";
+        case PQ_BAD_WIDTH: return "a dictionary-id bit width above 32";
+        case PQ_LEVELS_PAST_END: return "the definition levels run past the end of the page";
+        case PQ_TOO_MANY_RUNS: return "more runs than the stream's bytes allow";
+        default: return "malformed page";
+    }
+}
+
+}  // namespace
+}  // namespace vr
+
+using namespace vr;
+
+struct vr_pq_decoder {
+    int device = 0;
+    cudaStream_t own = nullptr;
+    int64_t max_values = 0, max_bytes = 0;
+    PqDev* pages_dev = nullptr;
+    PqDev* pages_host = nullptr;  // pinned
+    int pages_cap = 0;
+    RunEntry* runs = nullptr;
+    int64_t runs_cap = 0;
+    uint8_t* present = nullptr;
+    int32_t* rank = nullptr;
+    int32_t* compact = nullptr;
+    void* scan_tmp = nullptr;
+    size_t scan_bytes = 0;
+    int32_t* status_dev = nullptr;
+    int32_t* status_host = nullptr;  // pinned: reason, page, present (u64)
+    cudaEvent_t done = nullptr;
+    bool pending = false;
+    int last_pages = 0;
+};
+
+namespace {
+
+int pq_err(int code, const std::string& msg) {
+    vr::set_thread_error(msg);
+    return code;
+}
+
+int cuda_err(cudaError_t e, const char* what) {
+    return pq_err(VR_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// Run-table entries a stream of a page may need: at most one per two bytes
+// of the page (a run is a header and at least one byte of value or
+// payload), plus the entries long runs split into, plus the terminator.
+int64_t stream_cap(const vr_pq_page& pg) {
+    const int64_t n = pg.num_values;
+    return std::min<int64_t>(n, pg.length / 2 + n / kChunk + 2) + 2;
+}
+
+void free_all(vr_pq_decoder* d) {
+    cudaFree(d->pages_dev);
+    cudaFreeHost(d->pages_host);
+    cudaFree(d->runs);
+    cudaFree(d->present);
+    cudaFree(d->rank);
+    cudaFree(d->compact);
+    cudaFree(d->scan_tmp);
+    cudaFree(d->status_dev);
+    cudaFreeHost(d->status_host);
+    if (d->done) cudaEventDestroy(d->done);
+    if (d->own) cudaStreamDestroy(d->own);
+}
+
+}  // namespace
+
+extern "C" {
+
+int vr_pq_create(int32_t device, int64_t max_values, int64_t max_bytes, vr_pq_decoder** out) {
+    if (!out || max_values < 0 || max_bytes < 0 || max_values >= ((int64_t)1 << 31))
+        return pq_err(VR_ERR_INVALID, "vr_pq_create: bad argument (max_values must be below 2^31)");
+    *out = nullptr;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return cuda_err(e, "vr_pq_create");
+    auto* d = new vr_pq_decoder;
+    d->device = device;
+    d->max_values = max_values;
+    d->max_bytes = max_bytes;
+    const size_t n = (size_t)std::max<int64_t>(max_values, 1);
+    bool ok = cudaStreamCreateWithFlags(&d->own, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreateWithFlags(&d->done, cudaEventDisableTiming) == cudaSuccess &&
+              cudaMalloc(&d->present, n) == cudaSuccess && cudaMalloc(&d->rank, n * 4) == cudaSuccess &&
+              cudaMalloc(&d->compact, n * 4) == cudaSuccess && cudaMalloc(&d->status_dev, 16) == cudaSuccess &&
+              cudaMallocHost(&d->status_host, 16) == cudaSuccess;
+    if (ok) {
+        auto it = thrust::make_transform_iterator(static_cast<const uint8_t*>(d->present), ToInt());
+        ok = cub::DeviceScan::ExclusiveSum(nullptr, d->scan_bytes, it, d->rank, (int)n) == cudaSuccess &&
+             cudaMalloc(&d->scan_tmp, std::max<size_t>(d->scan_bytes, 16)) == cudaSuccess;
+    }
+    if (!ok) {
+        free_all(d);
+        delete d;
+        cudaGetLastError();
+        return pq_err(VR_ERR_OOM, "vr_pq_create: device allocation refused");
+    }
+    std::memset(d->status_host, 0, 16);
+    *out = d;
+    return VR_OK;
+}
+
+int vr_pq_decode(vr_pq_decoder* d, int32_t num_pages, const vr_pq_page* pages, void* out_data,
+                 uint8_t* out_validity, void* stream) {
+    if (!d || num_pages < 0 || (num_pages > 0 && (!pages || !out_data)))
+        return pq_err(VR_ERR_INVALID, "vr_pq_decode: null argument");
+    cudaSetDevice(d->device);
+    if (d->pending) {  // the pinned descriptors and status belong to the last call until it is done
+        cudaError_t e = cudaEventSynchronize(d->done);
+        if (e != cudaSuccess) return cuda_err(e, "vr_pq_decode");
+    }
+    int64_t slots = 0, bytes = 0, runs = 0;
+    bool levels = false;
+    const int enc = num_pages ? pages[0].encoding : 0;
+    const int vb = enc == VR_PQ_RLE_DICTIONARY ? 4 : (num_pages ? pages[0].value_bytes : 4);
+    for (int i = 0; i < num_pages; ++i) {
+        const vr_pq_page& pg = pages[i];
+        const std::string where = "vr_pq_decode: page " + std::to_string(i) + ": ";
+        if (!pg.data || pg.length < 0 || pg.num_values < 0 || pg.max_def_level < 0 || pg.levels_length < 0)
+            return pq_err(VR_ERR_INVALID, where + "bad descriptor");
+        if (pg.encoding != VR_PQ_PLAIN && pg.encoding != VR_PQ_RLE_DICTIONARY)
+            return pq_err(VR_ERR_UNSUPPORTED, where + "encoding other than PLAIN or RLE_DICTIONARY");
+        if (pg.encoding != enc)
+            return pq_err(VR_ERR_INVALID, where + "every page of one call must have the same encoding");
+        if (enc == VR_PQ_PLAIN && pg.value_bytes != vb)
+            return pq_err(VR_ERR_INVALID, where + "PLAIN pages of one call must have one value width");
+        if (vb != 4 && vb != 8) return pq_err(VR_ERR_UNSUPPORTED, where + "PLAIN values of 4 or 8 bytes only");
+        if (pg.length >= ((int64_t)1 << 32)) return pq_err(VR_ERR_UNSUPPORTED, where + "a page of 4 GiB or more");
+        levels |= pg.max_def_level > 0;
+        slots += pg.num_values;
+        bytes += pg.length;
+        runs += 2 * stream_cap(pg);
+    }
+    if (slots > d->max_values || bytes > d->max_bytes)
+        return pq_err(VR_ERR_INVALID, "vr_pq_decode: more slots or page bytes than the decoder was created for");
+    if (levels && !out_validity)
+        return pq_err(VR_ERR_INVALID, "vr_pq_decode: pages with definition levels need a validity buffer");
+    cudaStream_t st = stream ? (cudaStream_t)stream : d->own;
+    // grow the descriptor and run tables (rare: once per larger call)
+    if (num_pages > d->pages_cap) {
+        cudaStreamSynchronize(st);
+        cudaFree(d->pages_dev);
+        cudaFreeHost(d->pages_host);
+        d->pages_dev = nullptr;
+        d->pages_host = nullptr;
+        const int cap = std::max(num_pages, 2 * d->pages_cap);
+        if (cudaMalloc(&d->pages_dev, sizeof(PqDev) * cap) != cudaSuccess ||
+            cudaMallocHost(&d->pages_host, sizeof(PqDev) * cap) != cudaSuccess) {
+            d->pages_cap = 0;
+            cudaGetLastError();
+            return pq_err(VR_ERR_OOM, "vr_pq_decode: descriptor allocation refused");
+        }
+        d->pages_cap = cap;
+    }
+    if (runs > d->runs_cap) {
+        cudaStreamSynchronize(st);
+        cudaFree(d->runs);
+        d->runs = nullptr;
+        const int64_t cap = std::max(runs, d->runs_cap + d->runs_cap / 2);
+        if (cudaMalloc(&d->runs, sizeof(RunEntry) * cap) != cudaSuccess) {
+            d->runs_cap = 0;
+            cudaGetLastError();
+            return pq_err(VR_ERR_OOM, "vr_pq_decode: run table allocation refused");
+        }
+        d->runs_cap = cap;
+    }
+    int64_t slot = 0, rb = 0;
+    for (int i = 0; i < num_pages; ++i) {
+        const vr_pq_page& pg = pages[i];
+        PqDev& h = d->pages_host[i];
+        std::memset(&h, 0, sizeof(h));
+        h.data = pg.data;
+        h.length = pg.length;
+        h.slot_base = slot;
+        h.num_values = pg.num_values;
+        h.max_def = pg.max_def_level;
+        h.v2 = pg.v2;
+        h.levels_length = pg.levels_length;
+        h.encoding = pg.encoding;
+        h.value_bytes = vb;
+        const int64_t cap = stream_cap(pg);
+        for (int s = 0; s < 2; ++s) {
+            h.run_base[s] = rb;
+            h.run_cap[s] = (int32_t)cap;
+            rb += cap;
+        }
+        slot += pg.num_values;
+    }
+    d->pending = false;
+    d->last_pages = num_pages;
+    std::memset(d->status_host, 0, 16);
+    cudaError_t e = cudaMemsetAsync(d->status_dev, 0, 16, st);
+    if (num_pages > 0 && e == cudaSuccess)
+        e = cudaMemcpyAsync(d->pages_dev, d->pages_host, sizeof(PqDev) * num_pages, cudaMemcpyHostToDevice, st);
+    if (slots > 0 && e == cudaSuccess) {
+        if (levels) e = cudaMemsetAsync(d->present, 0, (size_t)slots, st);
+        if (e == cudaSuccess) {
+            k_pq_walk<<<num_pages, 64, 0, st>>>(d->pages_dev, d->runs, d->status_dev);
+            k_pq_expand<<<148 * 8, 256, 0, st>>>(d->pages_dev, num_pages, d->runs, d->present, d->compact,
+                                                  reinterpret_cast<int32_t*>(out_data));
+            e = cudaGetLastError();
+        }
+        if (levels && e == cudaSuccess) {
+            auto it = thrust::make_transform_iterator(static_cast<const uint8_t*>(d->present), ToInt());
+            size_t tb = d->scan_bytes;
+            e = cub::DeviceScan::ExclusiveSum(d->scan_tmp, tb, it, d->rank, (int)slots, st);
+        }
+        if (e == cudaSuccess) {
+            const int64_t blocks = (slots + 255) / 256;
+            k_pq_gather<<<(unsigned)blocks, 256, 0, st>>>(d->pages_dev, num_pages, slots, d->present, d->rank,
+                                                          d->compact, static_cast<uint8_t*>(out_data), vb,
+                                                          out_validity, d->status_dev);
+            e = cudaGetLastError();
+        }
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d->status_host, d->status_dev, 16, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaEventRecord(d->done, st);
+    if (e != cudaSuccess) return cuda_err(e, "vr_pq_decode");
+    d->pending = true;
+    return VR_OK;
+}
+
+int vr_pq_sync(vr_pq_decoder* d, int64_t* present) {
+    if (!d) return pq_err(VR_ERR_INVALID, "vr_pq_sync: null decoder");
+    cudaSetDevice(d->device);
+    if (d->pending) {
+        cudaError_t e = cudaEventSynchronize(d->done);
+        if (e != cudaSuccess) return cuda_err(e, "vr_pq_sync");
+        d->pending = false;
+    }
+    const int reason = d->status_host[0];
+    if (present) {
+        uint64_t n;
+        std::memcpy(&n, d->status_host + 2, 8);
+        *present = (int64_t)n;
+    }
+    if (reason)
+        return pq_err(VR_ERR_INVALID, "page " + std::to_string(d->status_host[1]) + ": " + reason_text(reason));
+    return VR_OK;
+}
+
+void vr_pq_destroy(vr_pq_decoder* d) {
+    if (!d) return;
+    cudaSetDevice(d->device);
+    if (d->pending) cudaEventSynchronize(d->done);
+    free_all(d);
+    delete d;
+}
+
+int vr_pq_plain_dictionary(const uint8_t* page, int64_t length, int32_t num_values, int32_t* offsets,
+                           uint8_t* data, int64_t* data_bytes) {
+    if ((!page && length > 0) || length < 0 || num_values < 0 || !data_bytes)
+        return pq_err(VR_ERR_INVALID, "vr_pq_plain_dictionary: bad argument");
+    int64_t at = 0, total = 0;
+    for (int32_t i = 0; i < num_values; ++i) {
+        if (length - at < 4) return pq_err(VR_ERR_INVALID, "dictionary page: entry " + std::to_string(i) +
+                                                               "'s length past the end of the page");
+        int32_t len;
+        std::memcpy(&len, page + at, 4);
+        at += 4;
+        if (len < 0 || len > length - at)
+            return pq_err(VR_ERR_INVALID, "dictionary page: entry " + std::to_string(i) + " past the end of the page");
+        if (offsets) offsets[i] = (int32_t)total;
+        if (data) std::memcpy(data + total, page + at, (size_t)len);
+        at += len;
+        total += len;
+        if (total >= ((int64_t)1 << 31)) return pq_err(VR_ERR_UNSUPPORTED, "dictionary page: 2 GiB of strings or more");
+    }
+    if (offsets) offsets[num_values] = (int32_t)total;
+    *data_bytes = total;
+    return VR_OK;
+}
+
+}  // extern "C"

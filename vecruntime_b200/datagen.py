@@ -21,7 +21,7 @@ Workloads (rows, keys, values, functions):
 from __future__ import annotations
 
 from dataclasses import dataclass
-from typing import List
+from typing import List, Optional
 
 import numpy as np
 
@@ -165,3 +165,79 @@ def input_bytes(w: Workload) -> int:
         if c.validity is not None:
             b += (w.rows + 7) // 8
     return b
+
+
+# ------------------------------------------------------------------ Parquet pages
+def _uleb(v: int) -> bytes:
+    out = bytearray()
+    while True:
+        b = v & 0x7F
+        v >>= 7
+        if v:
+            out.append(b | 0x80)
+        else:
+            out.append(b)
+            return bytes(out)
+
+
+def encode_hybrid(values: np.ndarray, width: int, max_groups: int = 63) -> bytes:
+    """Parquet's RLE / bit-packed hybrid encoding of `values` at `width`
+    bits, as a writer emits it: groups of 8 values (aligned from the
+    stream's start) that all hold one value and repeat the previous group's
+    value form RLE runs, the rest bit-packed runs of at most `max_groups`
+    groups; the last group is zero-padded (a reader stops at its count)."""
+    v = np.ascontiguousarray(values, dtype=np.uint32)
+    n = len(v)
+    if width == 0 or n == 0:
+        return b""
+    g = (n + 7) // 8
+    pad = np.zeros(g * 8, np.uint32)
+    pad[:n] = v
+    grp = pad.reshape(g, 8)
+    const = (grp == grp[:, :1]).all(axis=1)
+    const[-1] &= n % 8 == 0  # a padded last group is bit-packed
+    # bit-packed bytes of every group: width bytes each, LSB first
+    bits = ((pad[:, None] >> np.arange(width, dtype=np.uint32)) & 1).astype(np.uint8)
+    packed = np.packbits(bits.reshape(-1), bitorder="little").reshape(g, width)
+    first = grp[:, 0]
+    vbytes = (width + 7) // 8
+    out = []
+    i = 0
+    while i < g:
+        if const[i]:
+            j = i + 1
+            while j < g and const[j] and first[j] == first[i]:
+                j += 1
+            out.append(_uleb((j - i) * 8 << 1))
+            out.append(int(first[i]).to_bytes(4, "little")[:vbytes])
+        else:
+            j = i + 1
+            while j < g and j - i < max_groups and not const[j]:
+                j += 1
+            out.append(_uleb(((j - i) << 1) | 1))
+            out.append(packed[i:j].tobytes())
+        i = j
+    return b"".join(out)
+
+
+def dictionary_pages(ids: np.ndarray, nulls: Optional[np.ndarray], width: int, page_rows: int,
+                     v2: bool = False) -> list:
+    """A column chunk of RLE_DICTIONARY data pages for `ids` (a null slot
+    has no id in its page): [(page bytes, page fields)] with v1 or v2
+    framing and definition levels (max level 1) when `nulls` is given."""
+    out = []
+    n = len(ids)
+    for lo in range(0, n, page_rows):
+        hi = min(n, lo + page_rows)
+        present = np.ones(hi - lo, bool) if nulls is None else ~np.asarray(nulls[lo:hi], bool)
+        values = bytes([width]) + encode_hybrid(np.asarray(ids[lo:hi])[present], width)
+        lv = b"" if nulls is None else encode_hybrid(present.astype(np.uint32), 1)
+        if nulls is None:
+            page, ll = values, 0
+        elif v2:
+            page, ll = lv + values, len(lv)
+        else:
+            page, ll = len(lv).to_bytes(4, "little") + lv + values, 0
+        out.append((page, dict(num_values=hi - lo, max_def_level=0 if nulls is None else 1, v2=int(v2),
+                               levels_length=ll, encoding=1, value_bytes=4)))
+    return out

@@ -89,6 +89,15 @@ class AggSpec(C.Structure):
                 ("device", C.c_int32), ("flags", C.c_int32)]
 
 
+VR_PQ_PLAIN, VR_PQ_RLE_DICTIONARY = 0, 1
+
+
+class PqPage(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("length", C.c_int64), ("num_values", C.c_int32),
+                ("max_def_level", C.c_int32), ("v2", C.c_int32), ("levels_length", C.c_int32),
+                ("encoding", C.c_int32), ("value_bytes", C.c_int32)]
+
+
 class Dictionary(C.Structure):
     _fields_ = [("size", C.c_int32), ("reserved", C.c_int32), ("offsets", C.c_void_p), ("data", C.c_void_p),
                 ("validity", C.c_void_p), ("hashes", C.c_void_p)]
@@ -212,6 +221,11 @@ PROTOTYPES = [
     ("vr_srv_get_stats", C.c_int, [_P, C.POINTER(SrvStats)]),
     ("vr_srv_drain", C.c_int, [_P]),
     ("vr_srv_destroy", None, [_P]),
+    ("vr_pq_create", C.c_int, [C.c_int32, C.c_int64, C.c_int64, C.POINTER(_P)]),
+    ("vr_pq_decode", C.c_int, [_P, C.c_int32, C.POINTER(PqPage), _P, _P, _P]),
+    ("vr_pq_sync", C.c_int, [_P, C.POINTER(C.c_int64)]),
+    ("vr_pq_destroy", None, [_P]),
+    ("vr_pq_plain_dictionary", C.c_int, [_P, C.c_int64, C.c_int32, _P, _P, C.POINTER(C.c_int64)]),
 ]
 
 _lib = None
