@@ -69,6 +69,8 @@ PORT_NOTE = ("scalar C++ restatement of the reference's general-probe aggregate 
 # the launch-shape choice: what a DRAM byte count depends on
 KERNEL_SOURCES = ("agg_main.cuh", "agg_device.cuh", "agg_types.h", "vr_internal.h", "agg_kernels.cu", "batched.cu",
                   "jit.cpp", "plan.cpp", "abi.cu")
+# the page decoder's traffic depends on its own source alone
+PARQUET_SOURCES = ("parquet.cu",)
 
 # DRAM bytes (read + write) per aggregate launch, dram__bytes_read.sum +
 # dram__bytes_write.sum of one ncu capture, with the sha1 prefix of the
@@ -86,6 +88,7 @@ TRAFFIC = {
     "plain": ("92235e5bbdd0", 1 << 20, (25.449984e6 + 768) / 1e9, "exact"),
     "highcard": ("92235e5bbdd0", 8_000_000, (555.012608e6 + 186.404096e6) / 1e9, "approx"),
     "batched": ("92235e5bbdd0", 30_418_299, (1.313819e9 + 464.094464e6) / 1e9, "approx"),
+    "parquet": ("", 8 << 20, 0.0, "rows"),
 }
 
 
@@ -93,9 +96,9 @@ def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
 
-def kernel_sha() -> str:
+def kernel_sha(sources=KERNEL_SOURCES) -> str:
     h = hashlib.sha1()
-    for f in KERNEL_SOURCES:
+    for f in sources:
         with open(os.path.join(ROOT, "vecruntime_b200", "csrc", f), "rb") as fh:
             h.update(fh.read())
     return h.hexdigest()[:12]
@@ -108,7 +111,7 @@ def launch_traffic(name, rows):
     if t is None:
         return None, "no ncu capture of this workload"
     sha, at, gb, scaling = t
-    now = kernel_sha()
+    now = kernel_sha(PARQUET_SOURCES if name == "parquet" else KERNEL_SOURCES)
     if sha != now:
         return None, f"no ncu capture of the current kernel sources ({now}); the last one was taken on {sha or 'older sources'}"
     if rows == at:
@@ -522,6 +525,171 @@ def run_e2e(args, w, lib, device):
             "d2h_bytes_per_step": d2h, "ms_per_step": ms, "chunk_rows": chunk}
 
 
+# ------------------------------------------------------------------ Parquet pages
+PQ_ROWS, PQ_PAGE_ROWS, PQ_DICT, PQ_NULLS = 60_000_000, 1 << 20, 100_000, 0.01
+
+
+def parquet_chunk(rows):
+    """A dictionary-encoded string column chunk: ids uniform over 100,000
+    entries (17-bit), 1% nulls, v1 data pages of 2^20 slots."""
+    from vecruntime_b200 import datagen as G
+
+    rng = np.random.default_rng(G.SEEDS["parquet"])
+    ids = rng.integers(0, PQ_DICT, size=rows).astype(np.int32)
+    nulls = rng.random(rows) < PQ_NULLS
+    return G.dictionary_pages(ids, nulls, 17, PQ_PAGE_ROWS)
+
+
+def pq_pages_on(blob_ptr, pages):
+    from vecruntime_b200 import parquet as P
+
+    out, at = [], 0
+    for b, f in pages:
+        out.append(P.Page(blob_ptr + at, len(b), f["num_values"], f["max_def_level"], bool(f["v2"]),
+                          f["levels_length"], f["encoding"], f["value_bytes"]))
+        at += len(b)
+    return out
+
+
+def pq_oracle(pages, threads):
+    """The oracle's decode of every page (ParquetPageDecoder.decode restated),
+    pages spread over `threads` host threads: (ids, validity bits, seconds)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from oracle import pyoracle as O
+
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(threads) as ex:
+        res = list(ex.map(lambda pf: O.pq_decode_page(pf[0], **pf[1]), pages))
+    secs = time.perf_counter() - t0
+    ids = np.concatenate([r[0].view(np.int32) for r in res])
+    valid = np.concatenate([np.unpackbits(r[1], bitorder="little")[:f["num_values"]] for r, (_, f) in zip(res, pages)])
+    return ids, valid.astype(bool), secs
+
+
+def run_parquet(args, rank, world, device, check):
+    """Parquet feed: a 60M-slot column chunk's RLE_DICTIONARY data pages,
+    resident in HBM, decoded into Arrow ids + validity (vr_pq_decode)."""
+    import torch
+
+    from vecruntime_b200 import parquet as P
+
+    torch.cuda.set_device(device)
+    rows = args.rows if (args.rows and args.workload == "parquet") else PQ_ROWS
+    pages = parquet_chunk(rows)
+    blob = b"".join(b for b, _ in pages)
+    page_bytes = len(blob)
+    log(f"[rank {rank}] parquet: {rows} slots in {len(pages)} pages, {page_bytes / 1e6:.1f} MB")
+    dev = torch.device("cuda", device)
+    dblob = torch.frombuffer(bytearray(blob + b"\0" * 16), dtype=torch.uint8).to(dev)
+    dpages = pq_pages_on(dblob.data_ptr(), pages)
+    out = torch.empty(rows * 4 + 16, dtype=torch.uint8, device=dev)
+    vbytes = ((rows + 7) // 8 + 15) // 16 * 16 + 16
+    valid = torch.zeros(vbytes, dtype=torch.uint8, device=dev)
+    dec = P.PageDecoder(rows, page_bytes, device=device)
+    stream = torch.cuda.Stream(device=dev)
+    flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    for _ in range(args.warmup):
+        dec.decode(dpages, out.data_ptr(), valid.data_ptr(), stream.cuda_stream)
+        dec.sync()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    dist_barrier(world)
+    torch.cuda.synchronize(device)
+    present = 0
+    with ClockSampler(device) as clocks:
+        for i in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(i & 0xFF)
+            ev[i][0].record(stream)
+            dec.decode(dpages, out.data_ptr(), valid.data_ptr(), stream.cuda_stream)
+            ev[i][1].record(stream)
+            present = dec.sync()
+        torch.cuda.synchronize(device)
+    dist_barrier(world)
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    ms_per_step, value = weak_scaling(sum(step_ms), args.steps, rows, world, device)
+    parity = None
+    if check:
+        want_ids, want_valid, osecs = pq_oracle(pages, host_threads())
+        got_ids = out[:rows * 4].cpu().numpy().view(np.int32)
+        got_valid = np.unpackbits(valid.cpu().numpy(), bitorder="little")[:rows].astype(bool)
+        bad = int((got_ids != want_ids).sum() + (got_valid != want_valid).sum())
+        parity = {"slots": rows, "present": int(present), "oracle_present": int(want_valid.sum()),
+                  "mismatches": bad, "rule": "bit-exact ids and validity against the oracle's page decode",
+                  "oracle_s": round(osecs, 1)}
+    del flush
+    out_bytes = rows * 4 + (rows + 7) // 8
+    alg = page_bytes + out_bytes
+    peak, peak_kind = measured_peaks()
+    traffic, traffic_unit = launch_traffic("parquet", rows)
+    kernel_ms = float(np.mean(step_ms))
+    rec = {
+        "value": value, "unit": "rows/s", "ms_per_step": ms_per_step, "steps": args.steps, "warmup": args.warmup,
+        "dtype": "u8/u32 (bit unpacking)",
+        "config": {"workload": f"Parquet feed: {rows} slots of a dictionary-encoded string column (100,000 entries, "
+                               f"17-bit ids, 1% nulls) in {len(pages)} v1 RLE_DICTIONARY data pages of 2^20 slots "
+                               "-> Arrow int32 ids + validity",
+                   "rows_per_gpu": rows, "page_bytes": page_bytes, "pages": len(pages),
+                   "batch": "the column chunk's pages resident in HBM, one vr_pq_decode per step",
+                   "l2": "L2 flushed before each step (%d MB written on the stream outside the timed events)"
+                         % (FLUSH_BYTES >> 20)},
+        "roofline": {"bound": "hbm", "achieved": alg / (kernel_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": alg / (kernel_ms * 1e-3) / 1e9 / peak, "peak_kind": peak_kind,
+                     "traffic": traffic, "traffic_unit": traffic_unit, "algorithmic_bytes_per_launch": alg,
+                     "kernel_ms": kernel_ms, "kernel_ms_is": "the decode's kernels (run walk, expand, rank scan, gather)"},
+        "gpu_launches": 5 * args.steps,
+        "clocks": clocks.summary(),
+        "parity": parity,
+    }
+    if not args.no_e2e:
+        rec["e2e"] = run_parquet_e2e(args, dec, pages, blob, rows, device)
+        rec["e2e"]["value"] = dist_min(rec["e2e"]["value"], world, device) * world
+    if check and not args.no_cpu_baseline:
+        # the parity check's own decode: every page, timed
+        rec["cpu_baseline"] = {"value": rows / osecs, "unit": "rows/s", "cores": host_threads(), "kind": "port",
+                               "port": "scalar C++ restatement of the reference's ParquetPageDecoder.decode + "
+                                       "RleBitPackingReader.readInts (ids not resolved), one page per thread",
+                               "sample": f"all {len(pages)} pages ({rows} slots), {host_threads()} threads, "
+                                         f"{osecs:.2f} s"}
+    dec.close()
+    return rec
+
+
+def run_parquet_e2e(args, dec, pages, blob, rows, device):
+    """The same decode through the public API from host memory: every step
+    copies the pages from pinned host memory to the device, decodes them, and
+    copies the ids and validity back into pinned buffers."""
+    import torch
+
+    dev = torch.device("cuda", device)
+    hblob = torch.frombuffer(bytearray(blob + b"\0" * 16), dtype=torch.uint8).pin_memory()
+    dblob = torch.empty_like(hblob, device=dev)
+    dpages = pq_pages_on(dblob.data_ptr(), pages)
+    out = torch.empty(rows * 4 + 16, dtype=torch.uint8, device=dev)
+    vbytes = ((rows + 7) // 8 + 15) // 16 * 16 + 16
+    valid = torch.zeros(vbytes, dtype=torch.uint8, device=dev)
+    hout = torch.empty(rows * 4, dtype=torch.uint8).pin_memory()
+    hvalid = torch.empty((rows + 7) // 8, dtype=torch.uint8).pin_memory()
+    stream = torch.cuda.Stream(device=dev)
+    times = []
+    for it in range(max(1, args.warmup) + args.steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            a.record(stream)
+            dblob.copy_(hblob, non_blocking=True)
+            dec.decode(dpages, out.data_ptr(), valid.data_ptr(), stream.cuda_stream)
+            hout.copy_(out[:rows * 4], non_blocking=True)
+            hvalid.copy_(valid[:(rows + 7) // 8], non_blocking=True)
+            b.record(stream)
+        dec.sync()
+        torch.cuda.synchronize(device)
+        if it >= max(1, args.warmup):
+            times.append(a.elapsed_time(b))
+    ms = float(np.mean(times))
+    return {"value": rows / (ms * 1e-3), "unit": "rows/s", "h2d_bytes_per_step": len(blob),
+            "d2h_bytes_per_step": rows * 4 + (rows + 7) // 8, "ms_per_step": ms}
+
+
 # ------------------------------------------------------------------ batched
 def run_batched(args, rank, world, device, check):
     """512 uneven instances: one persistent launch replayed from a CUDA graph
@@ -899,7 +1067,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="all",
-                    choices=["all", "decimal", "plain", "highcard", "batched", "serving"])
+                    choices=["all", "decimal", "plain", "highcard", "batched", "serving", "parquet"])
     ap.add_argument("--instances", type=int, default=512, help="batched: instances")
     ap.add_argument("--rate", type=float, default=2000.0, help="serving: requests/s")
     ap.add_argument("--seconds", type=float, default=300.0, help="serving: trace length")
@@ -947,10 +1115,13 @@ def main():
         rec["workloads"] = {}
         for name in ("decimal", "highcard", "plain"):
             rec["workloads"][name] = run_single(args, name, rank, world, local, check)
+        rec["workloads"]["parquet"] = run_parquet(args, rank, world, local, check)
         if serving is not None:
             rec["serving"] = serving
     elif args.workload == "batched":
         rec = run_batched(args, rank, world, local, check)
+    elif args.workload == "parquet":
+        rec = run_parquet(args, rank, world, local, check)
     else:
         rec = run_single(args, args.workload, rank, world, local, check)
     if world > 1:

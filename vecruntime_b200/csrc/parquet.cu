@@ -96,76 +96,337 @@ __device__ uint32_t ld_le(const uint8_t* p, int n) {
 
 __device__ int width_of(int max_value) { return max_value ? 32 - __clz(max_value) : 0; }
 
-// Walks [pos, end) of page `d`'s bytes (lane 0 of the warp): run headers in
-// order, each bounds-checked with its payload, until `need` values are
-// covered or the stream stops. Returns the values covered.
-__device__ int64_t walk_stream(const uint8_t* base, int64_t pos, int64_t end, int w, int64_t need,
-                               RunEntry* runs, int32_t cap, int32_t& nruns) {
+// Bytes [pos, pos + 16) of a page as two little-endian words, bytes at or
+// past `end` read as 0 (and not loaded): 16 independent loads, one latency.
+__device__ void load16(const uint8_t* base, int64_t pos, int64_t end, uint64_t& lo, uint64_t& hi) {
+    lo = hi = 0;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        const uint64_t b = pos + i < end ? (uint64_t)__ldg(base + pos + i) : 0ull;
+        if (i < 8) lo |= b << (8 * i);
+        else hi |= b << (8 * (i - 8));
+    }
+}
+
+// The run whose header would start at page position q, from the 9 bytes at
+// q (x: bytes q..q+7, y: bytes q+8..): `step` = bytes to the next header
+// (0: no valid run starts here within [q, end)), `nvals` = its values
+// (clamped to 2^31 - 1), `word` = the RLE value or the page position of the
+// bit-packed payload.
+struct RunAt {
+    uint32_t step;
+    int32_t nvals;
+    uint32_t word;
+    bool packed;
+};
+__device__ RunAt run_at(uint64_t x, uint64_t y, int64_t q, int64_t end, int w, int vbytes, uint64_t vmask) {
+    RunAt r{0u, 0, 0u, false};
+    const int64_t avail = end - q;
+    if (avail <= 0) return r;
+    uint32_t h = 0;
+    int hl = 0;
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {  // ULEB128, at most 5 bytes (as the reference reads it)
+        const uint32_t b = (uint32_t)(x >> (8 * i)) & 0xFFu;
+        h |= (b & 0x7Fu) << (7 * i);
+        if (!(b & 0x80u)) {
+            hl = i + 1;
+            break;
+        }
+    }
+    if (hl == 0 || hl > avail) return r;  // a header cut by the end of the stream
+    const int64_t count = h >> 1;
+    r.packed = h & 1;
+    if (r.packed) {
+        const int64_t bytes = count * w;
+        if (hl + bytes > avail) return r;  // a bit-packed run past the end
+        r.step = (uint32_t)(hl + bytes);
+        r.nvals = (int32_t)(count * 8 < 0x7FFFFFFF ? count * 8 : 0x7FFFFFFF);
+        r.word = (uint32_t)(q + hl);
+    } else {
+        if (hl + vbytes > avail) return r;  // an RLE value past the end
+        const uint64_t z = (x >> (8 * hl)) | (y << (64 - 8 * hl));  // hl is 1..5
+        r.step = (uint32_t)(hl + vbytes);
+        r.nvals = (int32_t)(count < 0x7FFFFFFF ? count : 0x7FFFFFFF);
+        r.word = (uint32_t)(z & vmask);
+    }
+    return r;
+}
+
+// The walk's state in lane 0: entries written, values covered, no room left.
+struct Emit {
+    RunEntry* runs;
+    int32_t cap;
     int32_t k = 0;
     int64_t got = 0;
+    bool full = false;
+};
+
+constexpr int kWin = 256;  // bytes a warp decodes at once in dense mode (8 per lane)
+struct WinTable {
+    uint32_t step[kWin];
+    int32_t nvals[kWin];
+    uint32_t word[kWin];
+    uint8_t packed[kWin];
+    uint16_t jump[2][kWin];  // 2^r-hop successor within the window (>= kWin: leaves it)
+    uint8_t mark[kWin];      // on the chain from the window's first byte
+};
+
+// Inclusive warp prefix sum of a 64-bit value.
+__device__ int64_t warp_scan(int64_t v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const int64_t t = __shfl_up_sync(0xffffffffu, v, d);
+        if (lane >= d) v += t;
+    }
+    return v;
+}
+
+// Walks the run headers of [pos, end) in order until `need` values are
+// covered or the stream stops; the whole warp calls it and lane 0 writes the
+// run table. A header's position follows from the previous run, so the walk
+// is a chain. Two modes, switched by the runs just seen:
+//   sparse -- lane 0 reads one header at a time (long bit-packed runs: the
+//             next header is far away, one step per run);
+//   dense  -- the warp decodes, in parallel, a run at every byte position of
+//             the next 256 bytes into shared memory, and lane 0 follows the
+//             chain through that table (short runs, e.g. the definition
+//             levels of a column with scattered nulls: a table read and a few
+//             register operations per run instead of a dependent parse).
+// Returns the values covered, or -1 when the run table had no room.
+__device__ int64_t walk_stream(const uint8_t* base, int64_t pos, int64_t end, int w, int64_t need,
+                               RunEntry* runs, int32_t cap, int32_t& nruns, WinTable& T) {
+    const int lane = threadIdx.x & 31;
+    Emit E{runs, cap};
     if (w == 0) {  // every value is 0 and no byte is read
-        if (need > 0 && cap >= 2) {
-            runs[0] = RunEntry{0u, 0u};
-            k = 1;
-            got = need;
-        }
-    } else {
-        const int vbytes = (w + 7) >> 3;
-        while (got < need && pos < end) {
-            uint32_t h = 0;
-            bool ok = false;
-            for (int shift = 0; shift <= 28 && pos < end; shift += 7) {
-                const uint8_t b = __ldg(base + pos++);
-                h |= (uint32_t)(b & 0x7F) << shift;
-                if (!(b & 0x80)) {
-                    ok = true;
-                    break;
-                }
+        if (lane == 0) {
+            if (need > 0 && cap >= 2) {
+                runs[0] = RunEntry{0u, 0u};
+                E.k = 1;
+                E.got = need;
             }
-            if (!ok) break;  // a header cut by the end of the stream
-            const int64_t count = h >> 1;
-            const bool packed = h & 1;
-            int64_t nvals;
-            uint32_t word;
-            if (packed) {
-                const int64_t bytes = count * w;
-                if (pos + bytes > end) break;  // a bit-packed run past the end
-                nvals = count * 8;
-                word = (uint32_t)pos;
-                pos += bytes;
+            runs[E.k].begin = (uint32_t)E.got;
+            nruns = E.k;
+        }
+        return __shfl_sync(0xffffffffu, E.got, 0);
+    }
+    const int vbytes = (w + 7) >> 3;
+    const uint64_t vmask = vbytes == 4 ? 0xFFFFFFFFull : ((1ull << (8 * vbytes)) - 1);
+    bool dense = false, stop = false;
+    int64_t got = 0;
+    while (!stop && got < need && pos < end) {  // uniform: lane 0's state is broadcast each step
+        // the next 8 KiB of the stream into L2 while lane 0 works through this
+        // part (every 128-byte line, two per lane; addresses inside the stream
+        // only): each step of the chain then waits on L2, not DRAM
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const int64_t a = pos + 128 + 256 * lane + 128 * j;
+            if (a < end) asm volatile("prefetch.global.L2 [%0];" ::"l"(base + a));
+        }
+        if (!dense) {
+            // stride speculation: lane 0 reads the run at pos (step S); lane l
+            // reads the one that would start at pos + l * S. Writers emit long
+            // bit-packed runs of one size, so the guesses hold and one step
+            // covers 32 runs; lanes 0..m are right, m being the first lane
+            // whose run is not S bytes long (its own start was still right).
+            RunAt r{0u, 0, 0u, false};
+            uint64_t lo, hi;
+            if (lane == 0) {
+                load16(base, pos, end, lo, hi);
+                r = run_at(lo, hi, pos, end, w, vbytes, vmask);
+            }
+            const uint32_t S = __shfl_sync(0xffffffffu, r.step, 0);
+            if (S == 0) {
+                if (lane == 0) stop = true;
             } else {
-                if (pos + vbytes > end) break;  // an RLE value past the end
-                word = ld_le(base + pos, vbytes);
-                pos += vbytes;
-                nvals = count;
-            }
-            // entries of at most kChunk values, none past the values needed
-            for (int64_t off = 0; off < nvals && got < need; off += kChunk) {
-                if (k + 1 >= cap) {
-                    got = -1;  // no room (a malformed stream: valid ones fit by construction)
-                    break;
+                const int64_t q = pos + (int64_t)lane * S;
+                if (lane > 0 && q < end) {
+                    load16(base, q, end, lo, hi);
+                    r = run_at(lo, hi, q, end, w, vbytes, vmask);
                 }
-                runs[k++] = RunEntry{(uint32_t)got | (packed ? kPacked : 0u),
-                                     packed ? word + (uint32_t)(off / 8 * w) : word};
-                got += nvals - off < kChunk ? nvals - off : kChunk;
+                const uint32_t same = __ballot_sync(0xffffffffu, r.step == S);
+                const int m = ~same ? __ffs(~same) - 1 : 31;
+                const bool mine = lane <= m && r.step != 0;
+                const int64_t got0 = __shfl_sync(0xffffffffu, E.got, 0);
+                const int32_t k0 = __shfl_sync(0xffffffffu, E.k, 0);
+                const int64_t vsum = mine ? r.nvals : 0;
+                const int64_t vincl = warp_scan(vsum);
+                const int64_t b = got0 + vincl - vsum;
+                const int64_t cover = mine && b < need ? (r.nvals < need - b ? r.nvals : need - b) : 0;
+                const int64_t nent = (cover + kChunk - 1) / kChunk;
+                const int64_t eincl = warp_scan(nent);
+                const int64_t etotal = __shfl_sync(0xffffffffu, eincl, 31);
+                const int64_t vtotal = __shfl_sync(0xffffffffu, vincl, 31);
+                const bool full = k0 + etotal + 1 > cap;
+                if (!full) {
+                    int64_t e = k0 + eincl - nent;
+                    for (int64_t off = 0; off < cover; off += kChunk)
+                        runs[e++] = RunEntry{(uint32_t)(b + off) | (r.packed ? kPacked : 0u),
+                                             r.packed ? r.word + (uint32_t)(off / 8 * w) : r.word};
+                }
+                const uint32_t stm = __shfl_sync(0xffffffffu, r.step, m);
+                if (lane == 0) {
+                    if (full) {
+                        E.full = true;
+                        stop = true;
+                    } else {
+                        E.k = (int32_t)(k0 + etotal);
+                        E.got = got0 + vtotal;
+                        if (stm == 0) {
+                            stop = true;  // lane m's run is malformed, or the stream ended there
+                        } else {
+                            pos = pos + (int64_t)m * S + stm;
+                            dense = stm < 32;
+                        }
+                    }
+                }
             }
-            if (got < 0) break;
+        } else {
+            const int64_t ws = pos;
+            uint64_t lo, hi;
+            load16(base, ws + 8 * lane, end, lo, hi);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int sh = 8 * j;
+                const uint64_t x = sh ? (lo >> sh) | (hi << (64 - sh)) : lo;
+                const uint64_t y = sh ? hi >> sh : hi;
+                const int q = 8 * lane + j;
+                const RunAt r = run_at(x, y, ws + q, end, w, vbytes, vmask);
+                T.step[q] = r.step;
+                T.nvals[q] = r.nvals;
+                T.word[q] = r.word;
+                T.packed[q] = r.packed;
+            }
+            __syncwarp();
+            // the chain through the window, in parallel: pointer doubling marks
+            // every position reachable from byte 0 (a run is at least one byte,
+            // so 8 rounds cover the 256 bytes); chain order is position order
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int q = 8 * lane + j;
+                const uint32_t st = T.step[q];
+                T.jump[0][q] = (uint16_t)(st == 0 ? 0xFFFFu : (q + st < 0xFFFFu ? q + st : 0xFFFEu));
+                T.mark[q] = q == 0;
+            }
+            __syncwarp();
+            int cur = 0;
+            for (int r = 0; r < 8; ++r) {
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const int q = 8 * lane + j;
+                    const uint32_t t = T.jump[cur][q];
+                    if (T.mark[q] && t < kWin) T.mark[t] = 1;
+                }
+                __syncwarp();
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const int q = 8 * lane + j;
+                    const uint32_t t = T.jump[cur][q];
+                    T.jump[cur ^ 1][q] = t < kWin ? T.jump[cur][t] : (uint16_t)t;
+                }
+                __syncwarp();
+                cur ^= 1;
+            }
+            // this lane's chain runs: values, entries (runs split at kChunk), the last one
+            const int64_t got0 = __shfl_sync(0xffffffffu, E.got, 0);
+            const int32_t k0 = __shfl_sync(0xffffffffu, E.k, 0);
+            int64_t vsum = 0;
+            bool bad = false;
+            int last = -1;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int q = 8 * lane + j;
+                if (!T.mark[q]) continue;
+                if (T.step[q] == 0) bad = true;  // the chain stops here (malformed, or the stream ended)
+                else {
+                    vsum += T.nvals[q];
+                    last = q;
+                }
+            }
+            const int64_t vincl = warp_scan(vsum);
+            int64_t begin = got0 + vincl - vsum;  // values before this lane's first chain run
+            int64_t nent = 0;
+            {
+                int64_t b = begin;
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const int q = 8 * lane + j;
+                    if (!T.mark[q] || T.step[q] == 0) continue;
+                    if (b < need) {
+                        const int64_t cover = T.nvals[q] < need - b ? T.nvals[q] : need - b;
+                        nent += (cover + kChunk - 1) / kChunk;
+                    }
+                    b += T.nvals[q];
+                }
+            }
+            const int64_t eincl = warp_scan(nent);
+            const int64_t etotal = __shfl_sync(0xffffffffu, eincl, 31);
+            const int64_t vtotal = __shfl_sync(0xffffffffu, vincl, 31);
+            const bool full = k0 + etotal + 1 > cap;
+            if (!full) {
+                int64_t e = k0 + eincl - nent;
+                int64_t b = begin;
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const int q = 8 * lane + j;
+                    if (!T.mark[q] || T.step[q] == 0) continue;
+                    const bool pk = T.packed[q] != 0;
+                    const uint32_t wd = T.word[q];
+                    const int64_t cover = b < need ? (T.nvals[q] < need - b ? T.nvals[q] : need - b) : 0;
+                    for (int64_t off = 0; off < cover; off += kChunk)
+                        runs[e++] = RunEntry{(uint32_t)(b + off) | (pk ? kPacked : 0u),
+                                             pk ? wd + (uint32_t)(off / 8 * w) : wd};
+                    b += T.nvals[q];
+                }
+            }
+            // the chain's exit: past its last run in the window
+            int qlast = last;
+#pragma unroll
+            for (int d = 16; d > 0; d >>= 1) qlast = max(qlast, __shfl_xor_sync(0xffffffffu, qlast, d));
+            const bool any_bad = __any_sync(0xffffffffu, bad);
+            if (lane == 0) {
+                if (full) {
+                    E.full = true;
+                    stop = true;
+                } else {
+                    E.k = (int32_t)(k0 + etotal);
+                    E.got = got0 + vtotal;
+                    stop = any_bad;
+                    if (qlast >= 0) {
+                        const int64_t exit = qlast + (int64_t)T.step[qlast];
+                        pos = ws + exit;
+                        dense = exit < kWin + 64;  // the chain left the window by a long jump: back to sparse
+                    } else {
+                        stop = true;
+                    }
+                }
+            }
+            __syncwarp();
+        }
+        pos = __shfl_sync(0xffffffffu, pos, 0);
+        got = __shfl_sync(0xffffffffu, E.got, 0);
+        stop = __shfl_sync(0xffffffffu, stop, 0);
+        dense = __shfl_sync(0xffffffffu, dense, 0);
+    }
+    if (lane == 0) {
+        if (E.full) {
+            nruns = 0;
+        } else {
+            runs[E.k].begin = (uint32_t)(E.got < need ? E.got : need);  // terminator: the end of the last run
+            nruns = E.k;
         }
     }
-    if (got < 0) {
-        nruns = 0;
-        return -1;
-    }
-    const int64_t cover = got < need ? got : need;
-    runs[k].begin = (uint32_t)cover;  // terminator: the end of the last run
-    nruns = k;
-    return cover;
+    const bool full = __shfl_sync(0xffffffffu, E.full, 0);
+    return full ? -1 : (got < need ? got : need);
 }
 
 __global__ void k_pq_walk(PqDev* __restrict__ pages, RunEntry* __restrict__ runs, int32_t* __restrict__ status) {
+    __shared__ WinTable tables[2];
     const int p = blockIdx.x;
-    const int s = threadIdx.x >> 5;  // 0: definition levels, 1: values
-    if ((threadIdx.x & 31) != 0) return;
+    const int s = threadIdx.x >> 5;  // warp 0: definition levels, warp 1: values
+    const bool lead = (threadIdx.x & 31) == 0;
+    WinTable& T = tables[s];
     PqDev& d = pages[p];
     const uint8_t* base = d.data;
     int64_t lstart = 0, llen = 0;
@@ -174,60 +435,72 @@ __global__ void k_pq_walk(PqDev* __restrict__ pages, RunEntry* __restrict__ runs
             llen = d.levels_length;
         } else {
             if (d.length < 4) {
-                if (s == 0) pq_fail(status, PQ_LEVELS_PAST_END, p);
+                if (s == 0 && lead) pq_fail(status, PQ_LEVELS_PAST_END, p);
                 return;
             }
             lstart = 4;
             llen = (int32_t)ld_le(base, 4);
         }
         if (llen < 0 || lstart + llen > d.length) {
-            if (s == 0) pq_fail(status, PQ_LEVELS_PAST_END, p);
+            if (s == 0 && lead) pq_fail(status, PQ_LEVELS_PAST_END, p);
             return;
         }
     }
     const int64_t vstart = lstart + llen;
+    int32_t nr = 0;
     if (s == 0) {
-        d.values_start = vstart;
+        if (lead) d.values_start = vstart;
         if (d.max_def == 0) {
-            d.runs[0] = 0;
-            d.decoded[0] = d.num_values;
+            if (lead) {
+                d.runs[0] = 0;
+                d.decoded[0] = d.num_values;
+            }
             return;
         }
         const int w = width_of(d.max_def);
-        d.width[0] = w;
-        int32_t nr = 0;
         const int64_t got = walk_stream(base, lstart, lstart + llen, w, d.num_values, runs + d.run_base[0],
-                                        d.run_cap[0], nr);
-        d.runs[0] = nr;
-        d.decoded[0] = got < 0 ? 0 : (int32_t)got;
-        if (got < 0) pq_fail(status, PQ_TOO_MANY_RUNS, p);
-        else if (got < d.num_values) pq_fail(status, PQ_LEVELS_SHORT, p);
+                                        d.run_cap[0], nr, T);
+        if (lead) {
+            d.width[0] = w;
+            d.runs[0] = nr;
+            d.decoded[0] = got < 0 ? 0 : (int32_t)got;
+            if (got < 0) pq_fail(status, PQ_TOO_MANY_RUNS, p);
+            else if (got < d.num_values) pq_fail(status, PQ_LEVELS_SHORT, p);
+        }
         return;
     }
     if (d.encoding != VR_PQ_RLE_DICTIONARY) {  // PLAIN: the values region is the values
-        d.runs[1] = 0;
-        const int64_t avail = (d.length - vstart) / d.value_bytes;
-        d.decoded[1] = (int32_t)(avail < d.num_values ? (avail < 0 ? 0 : avail) : d.num_values);
+        if (lead) {
+            d.runs[1] = 0;
+            const int64_t avail = (d.length - vstart) / d.value_bytes;
+            d.decoded[1] = (int32_t)(avail < d.num_values ? (avail < 0 ? 0 : avail) : d.num_values);
+        }
         return;
     }
     if (vstart >= d.length) {  // no id bit width byte
-        d.runs[1] = 0;
-        d.decoded[1] = 0;
+        if (lead) {
+            d.runs[1] = 0;
+            d.decoded[1] = 0;
+        }
         return;
     }
     const int w = __ldg(base + vstart);
-    d.width[1] = w;
     if (w > 32) {
-        d.runs[1] = 0;
-        d.decoded[1] = 0;
-        pq_fail(status, PQ_BAD_WIDTH, p);
+        if (lead) {
+            d.runs[1] = 0;
+            d.decoded[1] = 0;
+            pq_fail(status, PQ_BAD_WIDTH, p);
+        }
         return;
     }
-    int32_t nr = 0;
-    const int64_t got = walk_stream(base, vstart + 1, d.length, w, d.num_values, runs + d.run_base[1], d.run_cap[1], nr);
-    d.runs[1] = nr;
-    d.decoded[1] = got < 0 ? 0 : (int32_t)got;
-    if (got < 0) pq_fail(status, PQ_TOO_MANY_RUNS, p);
+    const int64_t got = walk_stream(base, vstart + 1, d.length, w, d.num_values, runs + d.run_base[1], d.run_cap[1],
+                                    nr, T);
+    if (lead) {
+        d.width[1] = w;
+        d.runs[1] = nr;
+        d.decoded[1] = got < 0 ? 0 : (int32_t)got;
+        if (got < 0) pq_fail(status, PQ_TOO_MANY_RUNS, p);
+    }
 }
 
 // Value i of a bit-packed run whose payload starts at `payload`: its bits
@@ -295,43 +568,59 @@ __device__ int page_of(const PqDev* pages, int num_pages, int64_t i) {
     return lo;
 }
 
-// One thread per slot (warps on 32-slot boundaries, so each ballot is one
-// whole validity word).
+// Slots in a grid-stride loop, one per thread per step (warps on 32-slot
+// boundaries, so each ballot is one whole validity word); the present count
+// is summed per block and added once per block.
 __global__ void k_pq_gather(const PqDev* __restrict__ pages, int num_pages, int64_t n,
                             const uint8_t* __restrict__ present, const int32_t* __restrict__ rank,
                             const int32_t* __restrict__ compact, uint8_t* __restrict__ out, int vb,
                             uint8_t* __restrict__ validity, int32_t* __restrict__ status) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ unsigned long long block_present;
+    if (threadIdx.x == 0) block_present = 0;
+    __syncthreads();
     const int lane = threadIdx.x & 31;
-    bool valid = false;
-    if (i < n) {
-        const int p = page_of(pages, num_pages, i);
-        const PqDev& d = pages[p];
-        const bool levels = d.max_def > 0;
-        valid = levels ? present[i] != 0 : true;
-        const int64_t r = levels ? (int64_t)rank[i] - rank[d.slot_base] : i - d.slot_base;
-        uint8_t* dst = out + i * vb;
-        if (!valid) {
-            for (int j = 0; j < vb; ++j) dst[j] = 0;
-        } else if (r >= d.decoded[1]) {
-            for (int j = 0; j < vb; ++j) dst[j] = 0;
-            pq_fail(status, d.encoding == VR_PQ_RLE_DICTIONARY ? PQ_IDS_SHORT : PQ_PLAIN_SHORT, p);
-        } else if (d.encoding == VR_PQ_RLE_DICTIONARY) {
-            if (levels) reinterpret_cast<int32_t*>(out)[i] = compact[d.slot_base + r];
-        } else {
-            const uint8_t* src = d.data + d.values_start + r * vb;
-            for (int j = 0; j < vb; ++j) dst[j] = __ldg(src + j);
+    unsigned long long mine = 0;
+    for (int64_t first = (int64_t)blockIdx.x * blockDim.x; first < n; first += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = first + threadIdx.x;
+        // the warp's page, looked up once: a warp's 32 slots nearly always lie in one page
+        int p0 = lane == 0 && i < n ? page_of(pages, num_pages, i) : 0;
+        p0 = __shfl_sync(0xffffffffu, p0, 0);
+        const bool one_page = p0 + 1 >= num_pages || pages[p0 + 1].slot_base > i - lane + 31;
+        bool valid = false;
+        if (i < n) {
+            const int p = one_page ? p0 : page_of(pages, num_pages, i);
+            const PqDev& d = pages[p];
+            const bool levels = d.max_def > 0;
+            valid = levels ? present[i] != 0 : true;
+            const int64_t r = levels ? (int64_t)rank[i] - rank[d.slot_base] : i - d.slot_base;
+            uint8_t* dst = out + i * vb;
+            if (!valid) {
+                for (int j = 0; j < vb; ++j) dst[j] = 0;
+            } else if (r >= d.decoded[1]) {
+                for (int j = 0; j < vb; ++j) dst[j] = 0;
+                pq_fail(status, d.encoding == VR_PQ_RLE_DICTIONARY ? PQ_IDS_SHORT : PQ_PLAIN_SHORT, p);
+            } else if (d.encoding == VR_PQ_RLE_DICTIONARY) {
+                if (levels) reinterpret_cast<int32_t*>(out)[i] = compact[d.slot_base + r];
+            } else {
+                const uint8_t* src = d.data + d.values_start + r * vb;
+                for (int j = 0; j < vb; ++j) dst[j] = __ldg(src + j);
+            }
+        }
+        const uint32_t word = __ballot_sync(0xffffffffu, valid);
+        const int64_t wbase = i - lane;
+        if (lane == 0 && wbase < n) {
+            if (validity) {
+                const int64_t nbytes = (n + 7) >> 3;
+                for (int j = 0; j < 4 && (wbase >> 3) + j < nbytes; ++j)
+                    validity[(wbase >> 3) + j] = (uint8_t)(word >> (8 * j));
+            }
+            mine += __popc(word);
         }
     }
-    const uint32_t word = __ballot_sync(0xffffffffu, valid);
-    const int64_t base = i - lane;
-    if (lane == 0 && base < n) {
-        if (validity) {
-            const int64_t nbytes = (n + 7) >> 3;
-            for (int j = 0; j < 4 && (base >> 3) + j < nbytes; ++j) validity[(base >> 3) + j] = (uint8_t)(word >> (8 * j));
-        }
-        atomicAdd(reinterpret_cast<unsigned long long*>(status + 2), (unsigned long long)__popc(word));
-    }
+    if (lane == 0 && mine) atomicAdd(&block_present, mine);
+    __syncthreads();
+    if (threadIdx.x == 0 && block_present)
+        atomicAdd(reinterpret_cast<unsigned long long*>(status + 2), block_present);
 }
 
 const char* reason_text(int r) {
@@ -547,7 +836,7 @@ int vr_pq_decode(vr_pq_decoder* d, int32_t num_pages, const vr_pq_page* pages, v
             e = cub::DeviceScan::ExclusiveSum(d->scan_tmp, tb, it, d->rank, (int)slots, st);
         }
         if (e == cudaSuccess) {
-            const int64_t blocks = (slots + 255) / 256;
+            const int64_t blocks = std::min<int64_t>((slots + 255) / 256, 148 * 16);
             k_pq_gather<<<(unsigned)blocks, 256, 0, st>>>(d->pages_dev, num_pages, slots, d->present, d->rank,
                                                           d->compact, static_cast<uint8_t*>(out_data), vb,
                                                           out_validity, d->status_dev);

@@ -28,7 +28,7 @@ import numpy as np
 from . import aggregate as A
 from . import columns as Cc
 
-SEEDS = {"plain": 1001, "decimal": 1002, "highcard": 1003, "batched": 1004, "serving": 1005}
+SEEDS = {"plain": 1001, "decimal": 1002, "highcard": 1003, "batched": 1004, "serving": 1005, "parquet": 1006}
 
 
 @dataclass
