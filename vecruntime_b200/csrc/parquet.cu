@@ -164,10 +164,6 @@ struct Emit {
 
 constexpr int kWin = 256;  // bytes a warp decodes at once in dense mode (8 per lane)
 struct WinTable {
-    uint32_t step[kWin];
-    int32_t nvals[kWin];
-    uint32_t word[kWin];
-    uint8_t packed[kWin];
     uint16_t jump[2][kWin];  // 2^r-hop successor within the window (>= kWin: leaves it)
     uint8_t mark[kWin];      // on the chain from the window's first byte
 };
@@ -283,51 +279,54 @@ __device__ int64_t walk_stream(const uint8_t* base, int64_t pos, int64_t end, in
                 }
             }
         } else {
+            // this lane's 8 positions of the window: their runs stay in
+            // registers; only the jump table and the marks are shared
             const int64_t ws = pos;
             uint64_t lo, hi;
             load16(base, ws + 8 * lane, end, lo, hi);
+            RunAt R[8];
+            uint32_t J[8];
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
                 const int sh = 8 * j;
                 const uint64_t x = sh ? (lo >> sh) | (hi << (64 - sh)) : lo;
                 const uint64_t y = sh ? hi >> sh : hi;
                 const int q = 8 * lane + j;
-                const RunAt r = run_at(x, y, ws + q, end, w, vbytes, vmask);
-                T.step[q] = r.step;
-                T.nvals[q] = r.nvals;
-                T.word[q] = r.word;
-                T.packed[q] = r.packed;
+                R[j] = run_at(x, y, ws + q, end, w, vbytes, vmask);
+                J[j] = R[j].step == 0 ? 0xFFFFu : (q + R[j].step < 0xFFFFu ? q + R[j].step : 0xFFFEu);
+                T.jump[0][q] = (uint16_t)J[j];
+                T.mark[q] = q == 0;
             }
             __syncwarp();
             // the chain through the window, in parallel: pointer doubling marks
             // every position reachable from byte 0 (a run is at least one byte,
-            // so 8 rounds cover the 256 bytes); chain order is position order
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                const int q = 8 * lane + j;
-                const uint32_t st = T.step[q];
-                T.jump[0][q] = (uint16_t)(st == 0 ? 0xFFFFu : (q + st < 0xFFFFu ? q + st : 0xFFFEu));
-                T.mark[q] = q == 0;
-            }
-            __syncwarp();
+            // so 8 rounds cover the 256 bytes); chain order is position order.
+            // Each phase reads all 8 positions before it writes any, so the
+            // reads overlap.
             int cur = 0;
             for (int r = 0; r < 8; ++r) {
+                uint8_t mk[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) mk[j] = T.mark[8 * lane + j];
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                    if (mk[j] && J[j] < kWin) T.mark[J[j]] = 1;
+                if (r == 7) break;  // the last round's jumps are not needed
+                uint32_t N2[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) N2[j] = J[j] < kWin ? T.jump[cur][J[j]] : J[j];
 #pragma unroll
                 for (int j = 0; j < 8; ++j) {
-                    const int q = 8 * lane + j;
-                    const uint32_t t = T.jump[cur][q];
-                    if (T.mark[q] && t < kWin) T.mark[t] = 1;
-                }
-                __syncwarp();
-#pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    const int q = 8 * lane + j;
-                    const uint32_t t = T.jump[cur][q];
-                    T.jump[cur ^ 1][q] = t < kWin ? T.jump[cur][t] : (uint16_t)t;
+                    J[j] = N2[j];
+                    T.jump[cur ^ 1][8 * lane + j] = (uint16_t)N2[j];
                 }
                 __syncwarp();
                 cur ^= 1;
             }
+            __syncwarp();
+            bool on[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) on[j] = T.mark[8 * lane + j] != 0;
             // this lane's chain runs: values, entries (runs split at kChunk), the last one
             const int64_t got0 = __shfl_sync(0xffffffffu, E.got, 0);
             const int32_t k0 = __shfl_sync(0xffffffffu, E.k, 0);
@@ -336,28 +335,26 @@ __device__ int64_t walk_stream(const uint8_t* base, int64_t pos, int64_t end, in
             int last = -1;
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
-                const int q = 8 * lane + j;
-                if (!T.mark[q]) continue;
-                if (T.step[q] == 0) bad = true;  // the chain stops here (malformed, or the stream ended)
+                if (!on[j]) continue;
+                if (R[j].step == 0) bad = true;  // the chain stops here (malformed, or the stream ended)
                 else {
-                    vsum += T.nvals[q];
-                    last = q;
+                    vsum += R[j].nvals;
+                    last = 8 * lane + j;
                 }
             }
             const int64_t vincl = warp_scan(vsum);
-            int64_t begin = got0 + vincl - vsum;  // values before this lane's first chain run
+            const int64_t begin = got0 + vincl - vsum;  // values before this lane's first chain run
             int64_t nent = 0;
             {
                 int64_t b = begin;
 #pragma unroll
                 for (int j = 0; j < 8; ++j) {
-                    const int q = 8 * lane + j;
-                    if (!T.mark[q] || T.step[q] == 0) continue;
+                    if (!on[j] || R[j].step == 0) continue;
                     if (b < need) {
-                        const int64_t cover = T.nvals[q] < need - b ? T.nvals[q] : need - b;
+                        const int64_t cover = R[j].nvals < need - b ? R[j].nvals : need - b;
                         nent += (cover + kChunk - 1) / kChunk;
                     }
-                    b += T.nvals[q];
+                    b += R[j].nvals;
                 }
             }
             const int64_t eincl = warp_scan(nent);
@@ -369,21 +366,24 @@ __device__ int64_t walk_stream(const uint8_t* base, int64_t pos, int64_t end, in
                 int64_t b = begin;
 #pragma unroll
                 for (int j = 0; j < 8; ++j) {
-                    const int q = 8 * lane + j;
-                    if (!T.mark[q] || T.step[q] == 0) continue;
-                    const bool pk = T.packed[q] != 0;
-                    const uint32_t wd = T.word[q];
-                    const int64_t cover = b < need ? (T.nvals[q] < need - b ? T.nvals[q] : need - b) : 0;
+                    if (!on[j] || R[j].step == 0) continue;
+                    const int64_t cover = b < need ? (R[j].nvals < need - b ? R[j].nvals : need - b) : 0;
                     for (int64_t off = 0; off < cover; off += kChunk)
-                        runs[e++] = RunEntry{(uint32_t)(b + off) | (pk ? kPacked : 0u),
-                                             pk ? wd + (uint32_t)(off / 8 * w) : wd};
-                    b += T.nvals[q];
+                        runs[e++] = RunEntry{(uint32_t)(b + off) | (R[j].packed ? kPacked : 0u),
+                                             R[j].packed ? R[j].word + (uint32_t)(off / 8 * w) : R[j].word};
+                    b += R[j].nvals;
                 }
             }
             // the chain's exit: past its last run in the window
             int qlast = last;
+            uint32_t slast = 0;  // the step of this lane's last chain run
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+                if (8 * lane + j == last) slast = R[j].step;
 #pragma unroll
             for (int d = 16; d > 0; d >>= 1) qlast = max(qlast, __shfl_xor_sync(0xffffffffu, qlast, d));
+            const int owner = qlast >= 0 ? qlast >> 3 : 0;
+            const uint32_t stl = __shfl_sync(0xffffffffu, slast, owner);
             const bool any_bad = __any_sync(0xffffffffu, bad);
             if (lane == 0) {
                 if (full) {
@@ -394,7 +394,7 @@ __device__ int64_t walk_stream(const uint8_t* base, int64_t pos, int64_t end, in
                     E.got = got0 + vtotal;
                     stop = any_bad;
                     if (qlast >= 0) {
-                        const int64_t exit = qlast + (int64_t)T.step[qlast];
+                        const int64_t exit = qlast + (int64_t)stl;
                         pos = ws + exit;
                         dense = exit < kWin + 64;  // the chain left the window by a long jump: back to sparse
                     } else {
