@@ -81,6 +81,8 @@ PARQUET_SOURCES = ("parquet.cu",)
 #               group count; scaled by rows from the smaller capture, so a
 #               little low (earlier sources: 93 B/row at 8M high-cardinality
 #               rows, 103 B/row at 100M);
+#   "l2"     -- scaled by rows from a capture whose intermediate arrays
+#               stayed in L2: a lower bound at sizes where they do not;
 #   "exact"  -- captured at the timed size.
 TRAFFIC = {
     # name: (kernel sources sha1 prefix, rows captured, GB per launch, scaling)
@@ -88,7 +90,9 @@ TRAFFIC = {
     "plain": ("92235e5bbdd0", 1 << 20, (25.449984e6 + 768) / 1e9, "exact"),
     "highcard": ("92235e5bbdd0", 8_000_000, (555.012608e6 + 186.404096e6) / 1e9, "approx"),
     "batched": ("92235e5bbdd0", 30_418_299, (1.313819e9 + 464.094464e6) / 1e9, "approx"),
-    "parquet": ("", 8 << 20, 0.0, "rows"),
+    # the walk, expand and gather kernels (the CUB rank scan not captured)
+    "parquet": ("93e95684658c", 8 << 20, (6.475776e6 + 19.367424e6 + 0.331008e6 + 75.174144e6 + 9.979136e6) / 1e9,
+                "l2"),
 }
 
 
@@ -118,6 +122,9 @@ def launch_traffic(name, rows):
         return gb, f"GB per launch ({src}, capture of this workload on kernel sources {sha})"
     if scaling == "rows":
         return gb * rows / at, f"GB per launch ({src}, {at}-row capture on kernel sources {sha}, scaled by rows)"
+    if scaling == "l2":
+        return gb * rows / at, (f"GB per launch ({src}, {at}-row capture on kernel sources {sha}, scaled by rows; "
+                                "the capture's intermediates stayed in L2, so a lower bound)")
     if scaling == "approx":
         return gb * rows / at, (f"GB per launch ({src}, {at}-row capture on kernel sources {sha}, scaled by rows; "
                                 "table traffic per row grows slowly with groups, so a little low)")

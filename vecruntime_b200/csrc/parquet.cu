@@ -503,26 +503,15 @@ __global__ void k_pq_walk(PqDev* __restrict__ pages, RunEntry* __restrict__ runs
     }
 }
 
-// Value i of a bit-packed run whose payload starts at `payload`: its bits
-// lie in bytes [payload + i*w/8, payload + ceil((i+1)*w/8)), all inside the
-// run's checked payload.
-__device__ uint32_t packed_value(const uint8_t* payload, int64_t i, int w) {
-    const int64_t bit = i * w;
-    const uint8_t* b = payload + (bit >> 3);
-    const int sh = (int)(bit & 7);
-    const int nbytes = (sh + w + 7) >> 3;
-    uint64_t v = 0;
-    for (int j = 0; j < nbytes; ++j) v |= (uint64_t)__ldg(b + j) << (8 * j);
-    v >>= sh;
-    return (uint32_t)(w == 32 ? v : (v & ((1ull << w) - 1)));
-}
-
-// One warp per run, lanes over its values. present: a byte per slot;
+// One warp per run entry, lanes over its values (an RLE run) or its groups
+// of 8 (a bit-packed run). present: a byte per slot;
 // compact: a page's ids at slot_base + value index; out: the output column
 // (ids of pages without levels go there directly).
 __global__ void k_pq_expand(const PqDev* __restrict__ pages, int num_pages, const RunEntry* __restrict__ runs,
                             uint8_t* __restrict__ present, int32_t* __restrict__ compact, int32_t* __restrict__ out) {
+    __shared__ uint32_t stage[8][256];  // 256 threads per block: one 256-value stage per warp
     const int lane = threadIdx.x & 31;
+    uint32_t* sb = stage[threadIdx.x >> 5];
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int p = 0; p < num_pages; ++p) {
@@ -537,16 +526,47 @@ __global__ void k_pq_expand(const PqDev* __restrict__ pages, int num_pages, cons
                 const int64_t b0 = e.begin & ~kPacked;
                 const int64_t cnt = (int64_t)(R[k + 1].begin & ~kPacked) - b0;
                 const bool packed = (e.begin & kPacked) != 0;
-                const uint8_t* payload = d.data + e.word;
-                for (int64_t i = lane; i < cnt; i += 32) {
-                    const uint32_t v = packed ? packed_value(payload, i, w) : e.word;
-                    const int64_t slot = d.slot_base + b0 + i;
+                const int64_t slot0 = d.slot_base + b0;
+                auto put = [&](int64_t i, uint32_t v) {
                     if (s == 0)
-                        present[slot] = v == (uint32_t)d.max_def;
+                        present[slot0 + i] = v == (uint32_t)d.max_def;
                     else if (d.max_def > 0)
-                        compact[slot] = (int32_t)v;
+                        compact[slot0 + i] = (int32_t)v;
                     else
-                        out[slot] = (int32_t)v;
+                        out[slot0 + i] = (int32_t)v;
+                };
+                if (!packed) {
+                    for (int64_t i = lane; i < cnt; i += 32) put(i, e.word);
+                    continue;
+                }
+                // bit-packed: each lane unpacks one group of 8 (its w bytes,
+                // LSB first) into the warp's stage, then the warp stores the
+                // 256 values in order (coalesced)
+                const uint8_t* payload = d.data + e.word;
+                const uint64_t m = w == 32 ? 0xFFFFFFFFull : ((1ull << w) - 1);
+                const int64_t ng = (cnt + 7) >> 3;
+                for (int64_t g0 = 0; g0 < ng; g0 += 32) {
+                    const int64_t g = g0 + lane;
+                    if (g < ng) {
+                        const uint8_t* src = payload + g * w;
+                        uint64_t acc = 0;
+                        int bits = 0, nb = 0;
+#pragma unroll
+                        for (int v = 0; v < 8; ++v) {
+                            while (bits < w) {
+                                acc |= (uint64_t)__ldg(src + nb) << bits;
+                                ++nb;
+                                bits += 8;
+                            }
+                            sb[8 * lane + v] = (uint32_t)(acc & m);
+                            acc >>= w;
+                            bits -= w;
+                        }
+                    }
+                    __syncwarp();
+                    const int64_t here = cnt - 8 * g0 < 256 ? cnt - 8 * g0 : 256;
+                    for (int t = lane; t < here; t += 32) put(8 * g0 + t, sb[t]);
+                    __syncwarp();
                 }
             }
         }
