@@ -22,6 +22,11 @@ every other workload in one line:
   L2 is cold and the device is busy while the host submits the step. `e2e`
   goes through the public C ABI with pinned host buffers (chunked H2D
   overlapping the kernels, groups emitted into pinned buffers).
+* `workloads.parquet` -- the scan that feeds the aggregate: a 60M-slot
+  dictionary-encoded string column chunk (58 v1 RLE_DICTIONARY data pages,
+  17-bit ids, 1% nulls) resident in HBM, decoded into Arrow int32 ids and a
+  validity bitmap by one vr_pq_decode per step; parity is bit-exact against
+  the oracle's page decode, `e2e` copies the pages in and the column out.
 * `serving` -- 16 live queries fed by a seeded Poisson trace of 2,000
   requests/s for 5 minutes (one GPU): p50/p99 latency, queue wait, rows/s,
   the most requests in flight at once.
@@ -32,7 +37,7 @@ aggregate on the host cores, a bounded sample) and `parity`: after the timed
 steps, the groups of the full-size run are compared with the CPU port of the
 reference (groups as a sorted multiset; keys, counts, integer and decimal
 sums and min/max bit-exact; FP64 sums within 1e-12 relative of a compensated
-sum). --workload decimal|plain|highcard|batched|serving prints one of them as
+sum). --workload decimal|plain|highcard|batched|serving|parquet prints one of them as
 its own line; --impl reference times the CPU port on the host cores instead.
 
 Multi-GPU (torchrun): every rank aggregates its own replica (weak scaling, no

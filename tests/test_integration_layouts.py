@@ -12,7 +12,7 @@ from vecruntime_b200 import native as N
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 MIRRORS = {"COLUMN_TYPE": N.ColumnType, "DICTIONARY": N.Dictionary, "COLUMN": N.Column, "TERM": N.Term,
-           "AGG_FN": N.AggFn, "SPEC": N.AggSpec, "BATCH": N.Batch, "OUT_COLUMN": N.OutColumn}
+           "AGG_FN": N.AggFn, "SPEC": N.AggSpec, "BATCH": N.Batch, "OUT_COLUMN": N.OutColumn, "PQ_PAGE": N.PqPage}
 SIZES = {"JAVA_INT": 4, "JAVA_LONG": 8, "ADDRESS": 8}
 
 
@@ -50,7 +50,8 @@ def test_java_layout_matches_the_c_struct(name):
 
 
 C_NAMES = {"COLUMN_TYPE": "vr_column_type", "DICTIONARY": "vr_dictionary", "COLUMN": "vr_column", "TERM": "vr_term",
-           "AGG_FN": "vr_agg_fn", "SPEC": "vr_agg_spec", "BATCH": "vr_batch", "OUT_COLUMN": "vr_out_column"}
+           "AGG_FN": "vr_agg_fn", "SPEC": "vr_agg_spec", "BATCH": "vr_batch", "OUT_COLUMN": "vr_out_column",
+           "PQ_PAGE": "vr_pq_page"}
 
 
 def test_ctypes_mirrors_match_the_header(tmp_path):
