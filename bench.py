@@ -71,11 +71,13 @@ FLUSH_BYTES = 1 << 30  # written on the step's stream before each step's start e
 PORT_NOTE = ("scalar C++ restatement of the reference's general-probe aggregate (GroupKeyTable.lookupOrInsert + "
              "GroupedAccumulators), not its SIMD Vector API path; about half the reference's published per-core rate")
 # the kernels, the per-spec source generator, the planner (slot layout) and
-# the launch-shape choice: what a DRAM byte count depends on
-KERNEL_SOURCES = ("agg_main.cuh", "agg_device.cuh", "agg_types.h", "vr_internal.h", "agg_kernels.cu", "batched.cu",
-                  "jit.cpp", "plan.cpp", "abi.cu")
-# the page decoder's traffic depends on its own source alone
+# the launch-shape choice: what a DRAM byte count depends on (the batched
+# launch's also on batched.cu, the page decoder's on its own source alone)
+KERNEL_SOURCES = ("agg_main.cuh", "agg_device.cuh", "agg_types.h", "vr_internal.h", "agg_kernels.cu", "jit.cpp",
+                  "plan.cpp", "abi.cu")
+BATCHED_SOURCES = KERNEL_SOURCES + ("batched.cu",)
 PARQUET_SOURCES = ("parquet.cu",)
+TRAFFIC_SOURCES = {"batched": BATCHED_SOURCES, "parquet": PARQUET_SOURCES}
 
 # DRAM bytes (read + write) per aggregate launch, dram__bytes_read.sum +
 # dram__bytes_write.sum of one ncu capture, with the sha1 prefix of the
@@ -91,10 +93,10 @@ PARQUET_SOURCES = ("parquet.cu",)
 #   "exact"  -- captured at the timed size.
 TRAFFIC = {
     # name: (kernel sources sha1 prefix, rows captured, GB per launch, scaling)
-    "decimal": ("92235e5bbdd0", 8_000_000, (320.077568e6 + 7.250432e6) / 1e9, "rows"),
-    "plain": ("92235e5bbdd0", 1 << 20, (25.449984e6 + 768) / 1e9, "exact"),
-    "highcard": ("92235e5bbdd0", 8_000_000, (555.012608e6 + 186.404096e6) / 1e9, "approx"),
-    "batched": ("92235e5bbdd0", 30_418_299, (1.313819e9 + 464.094464e6) / 1e9, "approx"),
+    "decimal": ("c54880b41264", 8_000_000, (320.077568e6 + 7.250432e6) / 1e9, "rows"),
+    "plain": ("c54880b41264", 1 << 20, (25.449984e6 + 768) / 1e9, "exact"),
+    "highcard": ("c54880b41264", 8_000_000, (555.012608e6 + 186.404096e6) / 1e9, "approx"),
+    "batched": ("1d46e382ca92", 30_418_299, (1.659858e9 + 712.077568e6) / 1e9, "approx"),
     # the walk, expand and gather kernels (the CUB rank scan not captured)
     "parquet": ("93e95684658c", 8 << 20, (6.475776e6 + 19.367424e6 + 0.331008e6 + 75.174144e6 + 9.979136e6) / 1e9,
                 "l2"),
@@ -120,7 +122,7 @@ def launch_traffic(name, rows):
     if t is None:
         return None, "no ncu capture of this workload"
     sha, at, gb, scaling = t
-    now = kernel_sha(PARQUET_SOURCES if name == "parquet" else KERNEL_SOURCES)
+    now = kernel_sha(TRAFFIC_SOURCES.get(name, KERNEL_SOURCES))
     if sha != now:
         return None, f"no ncu capture of the current kernel sources ({now}); the last one was taken on {sha or 'older sources'}"
     if rows == at:

@@ -109,9 +109,12 @@ static int batched_enqueue(vr_batched* b, cudaStream_t st) {
 // Rows a producer takes per grab in the persistent launch (a run of
 // consecutive tiles of one instance), so a small instance is spread over
 // fewer CTAs, each of which flushes its shared-memory table into the
-// instance's HBM table. Measured on 512 uneven instances (1,024-row tiles):
-// one tile per grab 23.1 ms, 4 tiles 21.4, 8 20.2, 16 19.2, 32 18.7, 128 19.8.
-constexpr int kBatchedRunRows = 32768;
+// instance's HBM table. Measured on 512 uneven instances, 1,024-row tiles,
+// 256 consumer threads: one tile per grab 23.1 ms, 4 tiles 21.4, 8 20.2, 16
+// 19.2, 32 18.7, 128 19.8; with 512 consumer threads and the autotuner's
+// strategies: 16,384 rows per grab 15.0 ms, 32,768 13.7, 65,536 13.2,
+// 131,072 13.5.
+constexpr int kBatchedRunRows = 65536;
 
 // The persistent launch's block shape (hash tier): one for every instance,
 // since the stage layout and the kernel's thread count are per launch.
