@@ -421,13 +421,23 @@ __device__ int64_t walk_stream(const uint8_t* base, int64_t pos, int64_t end, in
     return full ? -1 : (got < need ? got : need);
 }
 
-__global__ void k_pq_walk(PqDev* __restrict__ pages, RunEntry* __restrict__ runs, int32_t* __restrict__ status) {
+// Slots per entry of the slot -> page table the gather starts its page
+// lookup from (entry j: the page holding slot j * kSlotBlock).
+constexpr int kSlotBlock = 1024;
+
+__global__ void k_pq_walk(PqDev* __restrict__ pages, RunEntry* __restrict__ runs, int32_t* __restrict__ status,
+                          int32_t* __restrict__ page_of_block) {
     __shared__ WinTable tables[2];
     const int p = blockIdx.x;
     const int s = threadIdx.x >> 5;  // warp 0: definition levels, warp 1: values
     const bool lead = (threadIdx.x & 31) == 0;
     WinTable& T = tables[s];
     PqDev& d = pages[p];
+    if (s == 0) {  // this page's entries of the slot -> page table
+        const int64_t lo = d.slot_base, hi = d.slot_base + d.num_values;
+        for (int64_t j = (lo + kSlotBlock - 1) / kSlotBlock + (threadIdx.x & 31); j * kSlotBlock < hi; j += 32)
+            page_of_block[j] = p;
+    }
     const uint8_t* base = d.data;
     int64_t lstart = 0, llen = 0;
     if (d.max_def > 0) {
@@ -507,18 +517,21 @@ __global__ void k_pq_walk(PqDev* __restrict__ pages, RunEntry* __restrict__ runs
 // of 8 (a bit-packed run). present: a byte per slot;
 // compact: a page's ids at slot_base + value index; out: the output column
 // (ids of pages without levels go there directly).
-__global__ void k_pq_expand(const PqDev* __restrict__ pages, int num_pages, const RunEntry* __restrict__ runs,
+__global__ void k_pq_expand(const PqDev* __restrict__ pages, int page0, const RunEntry* __restrict__ runs,
                             uint8_t* __restrict__ present, int32_t* __restrict__ compact, int32_t* __restrict__ out) {
     __shared__ uint32_t stage[8][256];  // 256 threads per block: one 256-value stage per warp
     const int lane = threadIdx.x & 31;
     uint32_t* sb = stage[threadIdx.x >> 5];
-    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int p = 0; p < num_pages; ++p) {
-        const PqDev& d = pages[p];
-        for (int s = 0; s < 2; ++s) {
+    // blocks (x, page, stream): the page's stream's runs over gridDim.x blocks of 8 warps
+    const int64_t warp = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int64_t nwarps = (int64_t)gridDim.x * 8;
+    const int p = page0 + (int)blockIdx.y;
+    const int s = (int)blockIdx.z;
+    const PqDev& d = pages[p];
+    {
+        {
             const int nr = d.runs[s];
-            if (s == 1 && d.encoding != VR_PQ_RLE_DICTIONARY) continue;
+            if (s == 1 && d.encoding != VR_PQ_RLE_DICTIONARY) return;
             const RunEntry* R = runs + d.run_base[s];
             const int w = d.width[s];
             for (int64_t k = warp; k < nr; k += nwarps) {
@@ -577,15 +590,13 @@ struct ToInt {
     __host__ __device__ int32_t operator()(uint8_t x) const { return x; }
 };
 
-// The page of slot i: the last page whose slot_base <= i.
-__device__ int page_of(const PqDev* pages, int num_pages, int64_t i) {
-    int lo = 0, hi = num_pages - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (pages[mid].slot_base <= i) lo = mid;
-        else hi = mid - 1;
-    }
-    return lo;
+// The page of slot i: the last page whose slot_base <= i, found from the
+// table entry of i's slot block by stepping forward over the pages that
+// start inside the block.
+__device__ int page_at(const PqDev* pages, int num_pages, const int32_t* page_of_block, int64_t i) {
+    int p = page_of_block[i / kSlotBlock];
+    while (p + 1 < num_pages && pages[p + 1].slot_base <= i) ++p;
+    return p;
 }
 
 // Slots in a grid-stride loop, one per thread per step (warps on 32-slot
@@ -594,7 +605,8 @@ __device__ int page_of(const PqDev* pages, int num_pages, int64_t i) {
 __global__ void k_pq_gather(const PqDev* __restrict__ pages, int num_pages, int64_t n,
                             const uint8_t* __restrict__ present, const int32_t* __restrict__ rank,
                             const int32_t* __restrict__ compact, uint8_t* __restrict__ out, int vb,
-                            uint8_t* __restrict__ validity, int32_t* __restrict__ status) {
+                            uint8_t* __restrict__ validity, int32_t* __restrict__ status,
+                            const int32_t* __restrict__ page_of_block) {
     __shared__ unsigned long long block_present;
     if (threadIdx.x == 0) block_present = 0;
     __syncthreads();
@@ -603,12 +615,12 @@ __global__ void k_pq_gather(const PqDev* __restrict__ pages, int num_pages, int6
     for (int64_t first = (int64_t)blockIdx.x * blockDim.x; first < n; first += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = first + threadIdx.x;
         // the warp's page, looked up once: a warp's 32 slots nearly always lie in one page
-        int p0 = lane == 0 && i < n ? page_of(pages, num_pages, i) : 0;
+        int p0 = lane == 0 && i < n ? page_at(pages, num_pages, page_of_block, i) : 0;
         p0 = __shfl_sync(0xffffffffu, p0, 0);
         const bool one_page = p0 + 1 >= num_pages || pages[p0 + 1].slot_base > i - lane + 31;
         bool valid = false;
         if (i < n) {
-            const int p = one_page ? p0 : page_of(pages, num_pages, i);
+            const int p = one_page ? p0 : page_at(pages, num_pages, page_of_block, i);
             const PqDev& d = pages[p];
             const bool levels = d.max_def > 0;
             valid = levels ? present[i] != 0 : true;
@@ -671,6 +683,7 @@ struct vr_pq_decoder {
     int64_t runs_cap = 0;
     uint8_t* present = nullptr;
     int32_t* rank = nullptr;
+    int32_t* page_of_block = nullptr;  // slot block -> page, one entry per kSlotBlock slots
     int32_t* compact = nullptr;
     void* scan_tmp = nullptr;
     size_t scan_bytes = 0;
@@ -706,6 +719,7 @@ void free_all(vr_pq_decoder* d) {
     cudaFree(d->runs);
     cudaFree(d->present);
     cudaFree(d->rank);
+    cudaFree(d->page_of_block);
     cudaFree(d->compact);
     cudaFree(d->scan_tmp);
     cudaFree(d->status_dev);
@@ -732,6 +746,7 @@ int vr_pq_create(int32_t device, int64_t max_values, int64_t max_bytes, vr_pq_de
     bool ok = cudaStreamCreateWithFlags(&d->own, cudaStreamNonBlocking) == cudaSuccess &&
               cudaEventCreateWithFlags(&d->done, cudaEventDisableTiming) == cudaSuccess &&
               cudaMalloc(&d->present, n) == cudaSuccess && cudaMalloc(&d->rank, n * 4) == cudaSuccess &&
+              cudaMalloc(&d->page_of_block, (n / kSlotBlock + 2) * 4) == cudaSuccess &&
               cudaMalloc(&d->compact, n * 4) == cudaSuccess && cudaMalloc(&d->status_dev, 16) == cudaSuccess &&
               cudaMallocHost(&d->status_host, 16) == cudaSuccess;
     if (ok) {
@@ -845,10 +860,18 @@ int vr_pq_decode(vr_pq_decoder* d, int32_t num_pages, const vr_pq_page* pages, v
     if (slots > 0 && e == cudaSuccess) {
         if (levels) e = cudaMemsetAsync(d->present, 0, (size_t)slots, st);
         if (e == cudaSuccess) {
-            k_pq_walk<<<num_pages, 64, 0, st>>>(d->pages_dev, d->runs, d->status_dev);
-            k_pq_expand<<<148 * 8, 256, 0, st>>>(d->pages_dev, num_pages, d->runs, d->present, d->compact,
-                                                  reinterpret_cast<int32_t*>(out_data));
-            e = cudaGetLastError();
+            k_pq_walk<<<num_pages, 64, 0, st>>>(d->pages_dev, d->runs, d->status_dev, d->page_of_block);
+            // blocks per (page, stream): enough warps for the largest page's
+            // runs, ~1 warp per 1,024 slots, 1 to 64 blocks of 8 warps
+            int64_t most = 1;
+            for (int i = 0; i < num_pages; ++i) most = std::max<int64_t>(most, pages[i].num_values);
+            const unsigned bx = (unsigned)std::min<int64_t>(64, std::max<int64_t>(1, (most + 8191) / 8192));
+            for (int p0 = 0; p0 < num_pages && e == cudaSuccess; p0 += 65535) {
+                const unsigned np = (unsigned)std::min(65535, num_pages - p0);
+                k_pq_expand<<<dim3(bx, np, 2), 256, 0, st>>>(d->pages_dev, p0, d->runs, d->present, d->compact,
+                                                              reinterpret_cast<int32_t*>(out_data));
+                e = cudaGetLastError();
+            }
         }
         if (levels && e == cudaSuccess) {
             auto it = thrust::make_transform_iterator(static_cast<const uint8_t*>(d->present), ToInt());
@@ -859,7 +882,7 @@ int vr_pq_decode(vr_pq_decoder* d, int32_t num_pages, const vr_pq_page* pages, v
             const int64_t blocks = std::min<int64_t>((slots + 255) / 256, 148 * 16);
             k_pq_gather<<<(unsigned)blocks, 256, 0, st>>>(d->pages_dev, num_pages, slots, d->present, d->rank,
                                                           d->compact, static_cast<uint8_t*>(out_data), vb,
-                                                          out_validity, d->status_dev);
+                                                          out_validity, d->status_dev, d->page_of_block);
             e = cudaGetLastError();
         }
     }

@@ -54,11 +54,19 @@ class PageDecoder:
         self.h = h
         self.device = device
 
-    def decode(self, pages: Sequence[Page], out_data: int, out_validity: Optional[int], stream: int = 0) -> None:
-        """Decodes `pages` (one column chunk, in order) into the device
-        buffers `out_data` (value_bytes per slot) and `out_validity`
-        (LSB-first bitmap); asynchronous on `stream`."""
-        arr = (N.PqPage * max(1, len(pages)))(*[p.ctypes() for p in pages])
+    @staticmethod
+    def descriptors(pages: Sequence[Page]):
+        """The pages as the vr_pq_page array the library reads: build it once
+        for a chunk decoded more than once (thousands of pages cost the
+        Python loop more than the decode)."""
+        return (N.PqPage * max(1, len(pages)))(*[p.ctypes() for p in pages])
+
+    def decode(self, pages, out_data: int, out_validity: Optional[int], stream: int = 0) -> None:
+        """Decodes `pages` (one column chunk, in order: Page objects or the
+        array `descriptors` returns) into the device buffers `out_data`
+        (value_bytes per slot) and `out_validity` (LSB-first bitmap);
+        asynchronous on `stream`."""
+        arr = pages if isinstance(pages, C.Array) else self.descriptors(pages)
         N.check(self._lib.vr_pq_decode(self.h, len(pages), arr, C.c_void_p(out_data),
                                        C.c_void_p(out_validity) if out_validity else None,
                                        C.c_void_p(stream) if stream else None), "vr_pq_decode")
