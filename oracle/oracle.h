@@ -75,6 +75,12 @@ int orc_pq_decode_page(const uint8_t* page, const vr_pq_page* desc, void* out_da
 int orc_pq_plain_dictionary(const uint8_t* page, int64_t length, int32_t num_values, int32_t* offsets,
                             uint8_t* data, int64_t* data_bytes);
 const char* orc_pq_last_error(void);
+/* Many pages of one chunk on `threads` host threads (the timed CPU
+ * baseline), each page into its own output: slots at slot_base[k], validity
+ * bytes at valid_base[k]. */
+int orc_pq_decode_pages_threads(int32_t num_pages, const uint8_t* const* pages, const vr_pq_page* descs,
+                                const int64_t* slot_base, const int64_t* valid_base, void* out_data,
+                                uint8_t* out_validity, int32_t threads, double* seconds);
 
 #ifdef __cplusplus
 }

@@ -18,9 +18,12 @@
  * whatever bytes follow in the page).
  */
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cstdint>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "oracle.h"
@@ -219,6 +222,39 @@ int orc_pq_plain_dictionary(const uint8_t* page, int64_t length, int32_t num_val
     if (offsets) offsets[num_values] = (int32_t)total;
     if (data_bytes) *data_bytes = total;
     return VR_OK;
+}
+
+// A column chunk's pages decoded on `threads` host threads, pages taken in
+// turn from a shared counter, each into its own output as the reference's
+// decoder produces one VectorBuffers per page: page k's slots at
+// out_data + slot_base[k] values, its validity bitmap at
+// out_validity + valid_base[k] bytes. The timed CPU baseline. Returns the
+// first error; *seconds = wall time of the decode.
+int orc_pq_decode_pages_threads(int32_t num_pages, const uint8_t* const* pages, const vr_pq_page* descs,
+                                const int64_t* slot_base, const int64_t* valid_base, void* out_data,
+                                uint8_t* out_validity, int32_t threads, double* seconds) {
+    std::atomic<int32_t> next{0};
+    std::atomic<int> err{VR_OK};
+    const int vb = num_pages && descs[0].encoding == VR_PQ_RLE_DICTIONARY ? 4 : (num_pages ? descs[0].value_bytes : 4);
+    auto work = [&]() {
+        for (int32_t k; (k = next.fetch_add(1)) < num_pages;) {
+            int64_t present = 0;
+            const int rc = orc_pq_decode_page(pages[k], &descs[k], static_cast<uint8_t*>(out_data) + slot_base[k] * vb,
+                                              out_validity + valid_base[k], &present);
+            if (rc) {
+                int expect = VR_OK;
+                err.compare_exchange_strong(expect, rc);
+                return;
+            }
+        }
+    };
+    const auto t0 = std::chrono::steady_clock::now();
+    std::vector<std::thread> pool;
+    for (int t = 1; t < std::max(1, threads); ++t) pool.emplace_back(work);
+    work();
+    for (auto& th : pool) th.join();
+    if (seconds) *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return err.load();
 }
 
 }  // extern "C"

@@ -55,6 +55,8 @@ def lib():
         L.orc_pq_decode_page.argtypes = [P, C.POINTER(N.PqPage), P, P, C.POINTER(C.c_int64)]
         L.orc_pq_plain_dictionary.argtypes = [P, C.c_int64, C.c_int32, P, P, C.POINTER(C.c_int64)]
         L.orc_pq_last_error.restype = C.c_char_p
+        L.orc_pq_decode_pages_threads.argtypes = [C.c_int32, P, C.POINTER(N.PqPage), P, P, P, P, C.c_int32,
+                                                  C.POINTER(C.c_double)]
         _lib = L
     return _lib
 
@@ -206,3 +208,26 @@ def pq_plain_dictionary(data: bytes, n: int):
     if rc:
         raise OracleError(rc, lib().orc_pq_last_error().decode())
     return offs, out[:total.value]
+
+
+def pq_decode_pages_threads(pages, threads: int):
+    """Every page of a chunk decoded on `threads` host threads, each into its
+    own output (as the reference's decoder returns one buffer set per page):
+    (slot bytes of all pages in order, per-page validity bitmaps, seconds)."""
+    n = len(pages)
+    blobs = [C.create_string_buffer(bytes(b) + b"\0" * 8, len(b) + 8) for b, _ in pages]
+    ptrs = (C.c_void_p * max(1, n))(*[C.cast(b, C.c_void_p) for b in blobs])
+    descs = (N.PqPage * max(1, n))(*[N.PqPage(None, len(b), **f) for b, f in pages])
+    counts = np.array([f["num_values"] for _, f in pages], np.int64)
+    vb = 4 if n and pages[0][1]["encoding"] == N.VR_PQ_RLE_DICTIONARY else (pages[0][1]["value_bytes"] if n else 4)
+    slot_base = np.concatenate([[0], np.cumsum(counts)[:-1]]).astype(np.int64) if n else np.zeros(1, np.int64)
+    vbytes = (counts + 7) // 8
+    valid_base = np.concatenate([[0], np.cumsum(vbytes)[:-1]]).astype(np.int64) if n else np.zeros(1, np.int64)
+    out = np.zeros(max(1, int(counts.sum())) * vb, np.uint8)
+    valid = np.zeros(max(1, int(vbytes.sum())), np.uint8)
+    secs = C.c_double()
+    rc = lib().orc_pq_decode_pages_threads(n, ptrs, descs, slot_base.ctypes.data, valid_base.ctypes.data,
+                                           out.ctypes.data, valid.ctypes.data, threads, C.byref(secs))
+    if rc:
+        raise OracleError(rc, lib().orc_pq_last_error().decode())
+    return out[:int(counts.sum()) * vb], valid, secs.value

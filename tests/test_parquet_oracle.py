@@ -118,3 +118,23 @@ def test_library_dictionary_page_matches_the_oracle():
     from vecruntime_b200 import native as NN
     with pytest.raises(NN.VrError, match="past the end"):
         P.dictionary_page(page[:-1], len(words))
+
+
+def test_threaded_page_decode_matches_page_by_page():
+    """The CPU baseline's threaded decode gives every page's slots and
+    validity exactly as the single-page decode does."""
+    from vecruntime_b200 import datagen as G
+
+    rng = np.random.default_rng(12)
+    ids = rng.integers(0, 3000, size=50_003).astype(np.int32)
+    nulls = rng.random(50_003) < 0.05
+    pages = G.dictionary_pages(ids, nulls, 12, 7_001)
+    out, valid, secs = O.pq_decode_pages_threads(pages, 4)
+    want = np.concatenate([O.pq_decode_page(b, **f)[0] for b, f in pages])
+    np.testing.assert_array_equal(out, want)
+    at = 0
+    for b, f in pages:
+        vb = (f["num_values"] + 7) // 8
+        np.testing.assert_array_equal(valid[at:at + vb], O.pq_decode_page(b, **f)[1][:vb])
+        at += vb
+    assert secs > 0
