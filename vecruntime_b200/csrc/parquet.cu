@@ -6,12 +6,13 @@
 //                   run headers of the definition levels and of the
 //                   dictionary ids, walked in order (each header's position
 //                   depends on the previous run), into a run table;
-//   2. k_pq_expand  one warp per run, lanes over its values: levels become
-//                   present flags (level == max_def_level), ids go to a
+//   2. k_pq_expand  one warp per run entry: levels become the bits of a
+//                   present bitmap (level == max_def_level), ids go to a
 //                   compact per-page array (or straight to the output when a
 //                   page has no levels);
-//   3. a CUB exclusive scan of the present flags: each slot's rank among the
-//                   present slots of the call;
+//   3. a CUB exclusive scan of the bitmap words' popcounts: a slot's rank
+//                   among the present slots is its word's prefix plus the
+//                   present bits below it;
 //   4. k_pq_gather  one thread per slot: the slot's id or PLAIN value (the
 //                   rank-th present value of its page), 0 at a null slot, and
 //                   the validity bitmap one warp ballot per 32 slots.
@@ -513,12 +514,58 @@ __global__ void k_pq_walk(PqDev* __restrict__ pages, RunEntry* __restrict__ runs
     }
 }
 
+// A level run entry's present slots (level == max_def) as bits of the call's
+// bitmap (zeroed before): an RLE run sets whole words with plain stores (no
+// other run touches a word its slots cover) and its end words with atomic
+// ORs; a bit-packed run's groups of 8 levels become 8 bits each, ORed into
+// the one or two words they land in.
+__device__ void levels_to_bits(const PqDev& d, const RunEntry& e, int64_t slot0, int64_t cnt, bool packed, int w,
+                               uint32_t* bits, int lane) {
+    if (!packed) {
+        if (e.word != (uint32_t)d.max_def) return;
+        const int64_t first = slot0 >> 5, last = (slot0 + cnt - 1) >> 5;
+        for (int64_t wd = first + lane; wd <= last; wd += 32) {
+            uint32_t m = 0xFFFFFFFFu;
+            if (wd == first) m &= 0xFFFFFFFFu << (slot0 & 31);
+            if (wd == last) m &= 0xFFFFFFFFu >> (31 - ((slot0 + cnt - 1) & 31));
+            if (m == 0xFFFFFFFFu) bits[wd] = m;
+            else atomicOr(&bits[wd], m);
+        }
+        return;
+    }
+    const uint8_t* payload = d.data + e.word;
+    const uint64_t mask = w == 32 ? 0xFFFFFFFFull : ((1ull << w) - 1);
+    const int64_t ng = (cnt + 7) >> 3;
+    for (int64_t g = lane; g < ng; g += 32) {
+        const uint8_t* src = payload + g * w;
+        uint64_t acc = 0;
+        int nbits = 0, nb = 0;
+        uint32_t b8 = 0;
+#pragma unroll
+        for (int v = 0; v < 8; ++v) {
+            while (nbits < w) {
+                acc |= (uint64_t)__ldg(src + nb) << nbits;
+                ++nb;
+                nbits += 8;
+            }
+            if (8 * g + v < cnt && (uint32_t)(acc & mask) == (uint32_t)d.max_def) b8 |= 1u << v;
+            acc >>= w;
+            nbits -= w;
+        }
+        if (!b8) continue;
+        const int64_t s0 = slot0 + 8 * g;
+        const int off = (int)(s0 & 31);
+        atomicOr(&bits[s0 >> 5], b8 << off);
+        if (off > 24) atomicOr(&bits[(s0 >> 5) + 1], b8 >> (32 - off));
+    }
+}
+
 // One warp per run entry, lanes over its values (an RLE run) or its groups
 // of 8 (a bit-packed run). present: a byte per slot;
 // compact: a page's ids at slot_base + value index; out: the output column
 // (ids of pages without levels go there directly).
 __global__ void k_pq_expand(const PqDev* __restrict__ pages, int page0, const RunEntry* __restrict__ runs,
-                            uint8_t* __restrict__ present, int32_t* __restrict__ compact, int32_t* __restrict__ out) {
+                            uint32_t* __restrict__ bits, int32_t* __restrict__ compact, int32_t* __restrict__ out) {
     __shared__ uint32_t stage[8][256];  // 256 threads per block: one 256-value stage per warp
     const int lane = threadIdx.x & 31;
     uint32_t* sb = stage[threadIdx.x >> 5];
@@ -540,10 +587,12 @@ __global__ void k_pq_expand(const PqDev* __restrict__ pages, int page0, const Ru
                 const int64_t cnt = (int64_t)(R[k + 1].begin & ~kPacked) - b0;
                 const bool packed = (e.begin & kPacked) != 0;
                 const int64_t slot0 = d.slot_base + b0;
+                if (s == 0) {  // levels: the present slots' bits of the call's bitmap
+                    levels_to_bits(d, e, slot0, cnt, packed, w, bits, lane);
+                    continue;
+                }
                 auto put = [&](int64_t i, uint32_t v) {
-                    if (s == 0)
-                        present[slot0 + i] = v == (uint32_t)d.max_def;
-                    else if (d.max_def > 0)
+                    if (d.max_def > 0)
                         compact[slot0 + i] = (int32_t)v;
                     else
                         out[slot0 + i] = (int32_t)v;
@@ -586,8 +635,8 @@ __global__ void k_pq_expand(const PqDev* __restrict__ pages, int page0, const Ru
     }
 }
 
-struct ToInt {
-    __host__ __device__ int32_t operator()(uint8_t x) const { return x; }
+struct PopCount {
+    __device__ uint32_t operator()(uint32_t x) const { return (uint32_t)__popc(x); }
 };
 
 // The page of slot i: the last page whose slot_base <= i, found from the
@@ -603,7 +652,7 @@ __device__ int page_at(const PqDev* pages, int num_pages, const int32_t* page_of
 // boundaries, so each ballot is one whole validity word); the present count
 // is summed per block and added once per block.
 __global__ void k_pq_gather(const PqDev* __restrict__ pages, int num_pages, int64_t n,
-                            const uint8_t* __restrict__ present, const int32_t* __restrict__ rank,
+                            const uint32_t* __restrict__ bits, const uint32_t* __restrict__ wpre,
                             const int32_t* __restrict__ compact, uint8_t* __restrict__ out, int vb,
                             uint8_t* __restrict__ validity, int32_t* __restrict__ status,
                             const int32_t* __restrict__ page_of_block) {
@@ -623,8 +672,13 @@ __global__ void k_pq_gather(const PqDev* __restrict__ pages, int num_pages, int6
             const int p = one_page ? p0 : page_at(pages, num_pages, page_of_block, i);
             const PqDev& d = pages[p];
             const bool levels = d.max_def > 0;
-            valid = levels ? present[i] != 0 : true;
-            const int64_t r = levels ? (int64_t)rank[i] - rank[d.slot_base] : i - d.slot_base;
+            // a slot's rank among the call's present slots: the prefix of its
+            // word plus the present bits below it in the word
+            auto rank_of = [&](int64_t x) {
+                return (int64_t)wpre[x >> 5] + __popc(bits[x >> 5] & ((1u << (x & 31)) - 1u));
+            };
+            valid = levels ? ((bits[i >> 5] >> (i & 31)) & 1u) != 0 : true;
+            const int64_t r = levels ? rank_of(i) - rank_of(d.slot_base) : i - d.slot_base;
             uint8_t* dst = out + i * vb;
             if (!valid) {
                 for (int j = 0; j < vb; ++j) dst[j] = 0;
@@ -681,8 +735,8 @@ struct vr_pq_decoder {
     int pages_cap = 0;
     RunEntry* runs = nullptr;
     int64_t runs_cap = 0;
-    uint8_t* present = nullptr;
-    int32_t* rank = nullptr;
+    uint32_t* bits = nullptr;  // the call's present slots, one bit per slot
+    uint32_t* wpre = nullptr;  // per bitmap word: present slots in the words before it
     int32_t* page_of_block = nullptr;  // slot block -> page, one entry per kSlotBlock slots
     int32_t* compact = nullptr;
     void* scan_tmp = nullptr;
@@ -717,8 +771,8 @@ void free_all(vr_pq_decoder* d) {
     cudaFree(d->pages_dev);
     cudaFreeHost(d->pages_host);
     cudaFree(d->runs);
-    cudaFree(d->present);
-    cudaFree(d->rank);
+    cudaFree(d->bits);
+    cudaFree(d->wpre);
     cudaFree(d->page_of_block);
     cudaFree(d->compact);
     cudaFree(d->scan_tmp);
@@ -745,13 +799,14 @@ int vr_pq_create(int32_t device, int64_t max_values, int64_t max_bytes, vr_pq_de
     const size_t n = (size_t)std::max<int64_t>(max_values, 1);
     bool ok = cudaStreamCreateWithFlags(&d->own, cudaStreamNonBlocking) == cudaSuccess &&
               cudaEventCreateWithFlags(&d->done, cudaEventDisableTiming) == cudaSuccess &&
-              cudaMalloc(&d->present, n) == cudaSuccess && cudaMalloc(&d->rank, n * 4) == cudaSuccess &&
+              cudaMalloc(&d->bits, (n / 32 + 2) * 4) == cudaSuccess &&
+              cudaMalloc(&d->wpre, (n / 32 + 2) * 4) == cudaSuccess &&
               cudaMalloc(&d->page_of_block, (n / kSlotBlock + 2) * 4) == cudaSuccess &&
               cudaMalloc(&d->compact, n * 4) == cudaSuccess && cudaMalloc(&d->status_dev, 16) == cudaSuccess &&
               cudaMallocHost(&d->status_host, 16) == cudaSuccess;
     if (ok) {
-        auto it = thrust::make_transform_iterator(static_cast<const uint8_t*>(d->present), ToInt());
-        ok = cub::DeviceScan::ExclusiveSum(nullptr, d->scan_bytes, it, d->rank, (int)n) == cudaSuccess &&
+        auto it = thrust::make_transform_iterator(static_cast<const uint32_t*>(d->bits), PopCount());
+        ok = cub::DeviceScan::ExclusiveSum(nullptr, d->scan_bytes, it, d->wpre, (int)(n / 32 + 2)) == cudaSuccess &&
              cudaMalloc(&d->scan_tmp, std::max<size_t>(d->scan_bytes, 16)) == cudaSuccess;
     }
     if (!ok) {
@@ -858,7 +913,8 @@ int vr_pq_decode(vr_pq_decoder* d, int32_t num_pages, const vr_pq_page* pages, v
     if (num_pages > 0 && e == cudaSuccess)
         e = cudaMemcpyAsync(d->pages_dev, d->pages_host, sizeof(PqDev) * num_pages, cudaMemcpyHostToDevice, st);
     if (slots > 0 && e == cudaSuccess) {
-        if (levels) e = cudaMemsetAsync(d->present, 0, (size_t)slots, st);
+        const int64_t words = (slots + 31) / 32;
+        if (levels) e = cudaMemsetAsync(d->bits, 0, (size_t)words * 4, st);
         if (e == cudaSuccess) {
             k_pq_walk<<<num_pages, 64, 0, st>>>(d->pages_dev, d->runs, d->status_dev, d->page_of_block);
             // blocks per (page, stream): enough warps for the largest page's
@@ -868,19 +924,19 @@ int vr_pq_decode(vr_pq_decoder* d, int32_t num_pages, const vr_pq_page* pages, v
             const unsigned bx = (unsigned)std::min<int64_t>(64, std::max<int64_t>(1, (most + 8191) / 8192));
             for (int p0 = 0; p0 < num_pages && e == cudaSuccess; p0 += 65535) {
                 const unsigned np = (unsigned)std::min(65535, num_pages - p0);
-                k_pq_expand<<<dim3(bx, np, 2), 256, 0, st>>>(d->pages_dev, p0, d->runs, d->present, d->compact,
+                k_pq_expand<<<dim3(bx, np, 2), 256, 0, st>>>(d->pages_dev, p0, d->runs, d->bits, d->compact,
                                                               reinterpret_cast<int32_t*>(out_data));
                 e = cudaGetLastError();
             }
         }
         if (levels && e == cudaSuccess) {
-            auto it = thrust::make_transform_iterator(static_cast<const uint8_t*>(d->present), ToInt());
+            auto it = thrust::make_transform_iterator(static_cast<const uint32_t*>(d->bits), PopCount());
             size_t tb = d->scan_bytes;
-            e = cub::DeviceScan::ExclusiveSum(d->scan_tmp, tb, it, d->rank, (int)slots, st);
+            e = cub::DeviceScan::ExclusiveSum(d->scan_tmp, tb, it, d->wpre, (int)words, st);
         }
         if (e == cudaSuccess) {
             const int64_t blocks = std::min<int64_t>((slots + 255) / 256, 148 * 16);
-            k_pq_gather<<<(unsigned)blocks, 256, 0, st>>>(d->pages_dev, num_pages, slots, d->present, d->rank,
+            k_pq_gather<<<(unsigned)blocks, 256, 0, st>>>(d->pages_dev, num_pages, slots, d->bits, d->wpre,
                                                           d->compact, static_cast<uint8_t*>(out_data), vb,
                                                           out_validity, d->status_dev, d->page_of_block);
             e = cudaGetLastError();
