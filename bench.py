@@ -98,7 +98,7 @@ TRAFFIC = {
     "highcard": ("c54880b41264", 8_000_000, (555.012608e6 + 186.404096e6) / 1e9, "approx"),
     "batched": ("1d46e382ca92", 30_418_299, (1.659858e9 + 712.077568e6) / 1e9, "approx"),
     # the walk, expand and gather kernels (the CUB rank scan not captured)
-    "parquet": ("ebc93dde26b4", 8 << 20, (8.64768e6 + 20.5312e6 + 35.43168e6 + 0.000256e6 + 0.1088e6 + 0.752896e6)
+    "parquet": ("4cc0acd4e6f3", 8 << 20, (8.64768e6 + 20.52864e6 + 35.454464e6 + 0.002048e6 + 0.084224e6 + 1.069056e6)
                 / 1e9, "l2"),
 }
 

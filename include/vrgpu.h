@@ -550,7 +550,9 @@ typedef struct vr_pq_page {
 
 typedef struct vr_pq_decoder vr_pq_decoder;
 /* A decoder on `device` for calls of up to `max_values` slots and
- * `max_bytes` page bytes in total (it sizes its device scratch for them). */
+ * `max_bytes` page bytes in total (it sizes its device scratch for them).
+ * One thread at a time per decoder; a call waits for the decoder's previous
+ * call before it reuses its scratch. */
 int vr_pq_create(int32_t device, int64_t max_values, int64_t max_bytes, vr_pq_decoder** out);
 /* Decodes `num_pages` pages of one column chunk, in order, into one column
  * of the pages' slots in order: out_data (device; value_bytes per slot) and

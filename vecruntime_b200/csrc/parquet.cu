@@ -8,14 +8,13 @@
 //                   depends on the previous run), into a run table;
 //   2. k_pq_expand  one warp per run entry: levels become the bits of a
 //                   present bitmap (level == max_def_level), ids go to a
-//                   compact per-page array (or straight to the output when a
-//                   page has no levels);
+//                   compact per-page array;
 //   3. a CUB exclusive scan of the bitmap words' popcounts: a slot's rank
 //                   among the present slots is its word's prefix plus the
 //                   present bits below it;
-//   4. k_pq_gather  one thread per slot: the slot's id or PLAIN value (the
-//                   rank-th present value of its page), 0 at a null slot, and
-//                   the validity bitmap one warp ballot per 32 slots.
+//   4. k_pq_gather  four slots per thread: each slot's id or PLAIN value
+//                   (the rank-th present value of its page), 0 at a null
+//                   slot, and the validity bitmap.
 //
 // Reference: ParquetPageDecoder.decode (parquet/src/main/java/io/vecruntime/
 // parquet/codec/ParquetPageDecoder.java:214-311) and RleBitPackingReader
@@ -562,10 +561,10 @@ __device__ void levels_to_bits(const PqDev& d, const RunEntry& e, int64_t slot0,
 
 // One warp per run entry, lanes over its values (an RLE run) or its groups
 // of 8 (a bit-packed run). present: a byte per slot;
-// compact: a page's ids at slot_base + value index; out: the output column
-// (ids of pages without levels go there directly).
+// bits: the call's present bitmap; compact: a page's ids at slot_base +
+// value index (the gather moves them to their slots).
 __global__ void k_pq_expand(const PqDev* __restrict__ pages, int page0, const RunEntry* __restrict__ runs,
-                            uint32_t* __restrict__ bits, int32_t* __restrict__ compact, int32_t* __restrict__ out) {
+                            uint32_t* __restrict__ bits, int32_t* __restrict__ compact) {
     __shared__ uint32_t stage[8][256];  // 256 threads per block: one 256-value stage per warp
     const int lane = threadIdx.x & 31;
     uint32_t* sb = stage[threadIdx.x >> 5];
@@ -591,12 +590,7 @@ __global__ void k_pq_expand(const PqDev* __restrict__ pages, int page0, const Ru
                     levels_to_bits(d, e, slot0, cnt, packed, w, bits, lane);
                     continue;
                 }
-                auto put = [&](int64_t i, uint32_t v) {
-                    if (d.max_def > 0)
-                        compact[slot0 + i] = (int32_t)v;
-                    else
-                        out[slot0 + i] = (int32_t)v;
-                };
+                auto put = [&](int64_t i, uint32_t v) { compact[slot0 + i] = (int32_t)v; };
                 if (!packed) {
                     for (int64_t i = lane; i < cnt; i += 32) put(i, e.word);
                     continue;
@@ -648,9 +642,14 @@ __device__ int page_at(const PqDev* pages, int num_pages, const int32_t* page_of
     return p;
 }
 
-// Slots in a grid-stride loop, one per thread per step (warps on 32-slot
-// boundaries, so each ballot is one whole validity word); the present count
-// is summed per block and added once per block.
+// Four consecutive slots per thread in a grid-stride loop (a block covers
+// 1,024 slots per step): the 4 slots share one bitmap word, so a thread
+// loads the word and its prefix once, finds each slot's rank with a
+// popcount, reads the 4 values (consecutive ranks of one page, or the
+// page's PLAIN values) and stores them with one 16-byte store where the
+// column is aligned. Lanes 8k..8k+7 of a warp cover one 32-slot validity
+// word, combined by shuffles. The present count is summed per block and
+// added once per block.
 __global__ void k_pq_gather(const PqDev* __restrict__ pages, int num_pages, int64_t n,
                             const uint32_t* __restrict__ bits, const uint32_t* __restrict__ wpre,
                             const int32_t* __restrict__ compact, uint8_t* __restrict__ out, int vb,
@@ -660,49 +659,75 @@ __global__ void k_pq_gather(const PqDev* __restrict__ pages, int num_pages, int6
     if (threadIdx.x == 0) block_present = 0;
     __syncthreads();
     const int lane = threadIdx.x & 31;
+    const bool aligned = ((uintptr_t)out & 15) == 0;
     unsigned long long mine = 0;
-    for (int64_t first = (int64_t)blockIdx.x * blockDim.x; first < n; first += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t i = first + threadIdx.x;
-        // the warp's page, looked up once: a warp's 32 slots nearly always lie in one page
-        int p0 = lane == 0 && i < n ? page_at(pages, num_pages, page_of_block, i) : 0;
-        p0 = __shfl_sync(0xffffffffu, p0, 0);
-        const bool one_page = p0 + 1 >= num_pages || pages[p0 + 1].slot_base > i - lane + 31;
-        bool valid = false;
-        if (i < n) {
-            const int p = one_page ? p0 : page_at(pages, num_pages, page_of_block, i);
-            const PqDev& d = pages[p];
-            const bool levels = d.max_def > 0;
-            // a slot's rank among the call's present slots: the prefix of its
-            // word plus the present bits below it in the word
-            auto rank_of = [&](int64_t x) {
-                return (int64_t)wpre[x >> 5] + __popc(bits[x >> 5] & ((1u << (x & 31)) - 1u));
-            };
-            valid = levels ? ((bits[i >> 5] >> (i & 31)) & 1u) != 0 : true;
-            const int64_t r = levels ? rank_of(i) - rank_of(d.slot_base) : i - d.slot_base;
-            uint8_t* dst = out + i * vb;
-            if (!valid) {
-                for (int j = 0; j < vb; ++j) dst[j] = 0;
-            } else if (r >= d.decoded[1]) {
-                for (int j = 0; j < vb; ++j) dst[j] = 0;
-                pq_fail(status, d.encoding == VR_PQ_RLE_DICTIONARY ? PQ_IDS_SHORT : PQ_PLAIN_SHORT, p);
-            } else if (d.encoding == VR_PQ_RLE_DICTIONARY) {
-                if (levels) reinterpret_cast<int32_t*>(out)[i] = compact[d.slot_base + r];
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x * 4;
+    for (int64_t first = (int64_t)blockIdx.x * blockDim.x * 4; first < n; first += stride) {
+        const int64_t i0 = first + 4 * (int64_t)threadIdx.x;
+        uint32_t nib = 0;
+        if (i0 < n) {
+            const uint32_t wbits = bits[i0 >> 5];
+            const uint32_t wp = wpre[i0 >> 5];
+            int p = page_at(pages, num_pages, page_of_block, i0);
+            uint64_t v[4] = {0, 0, 0, 0};
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int64_t i = i0 + j;
+                if (i >= n) break;
+                while (p + 1 < num_pages && pages[p + 1].slot_base <= i) ++p;
+                const PqDev& d = pages[p];
+                const bool levels = d.max_def > 0;
+                bool valid = true;
+                int64_t r = i - d.slot_base;
+                if (levels) {
+                    // a slot's rank among the call's present slots: its word's
+                    // prefix plus the present bits below it in the word
+                    const int64_t sb = d.slot_base;
+                    const int64_t rank0 = (int64_t)wpre[sb >> 5] + __popc(bits[sb >> 5] & ((1u << (sb & 31)) - 1u));
+                    valid = ((wbits >> (i & 31)) & 1u) != 0;
+                    r = (int64_t)wp + __popc(wbits & ((1u << (i & 31)) - 1u)) - rank0;
+                }
+                if (!valid) continue;
+                nib |= 1u << j;
+                if (r >= d.decoded[1]) {
+                    pq_fail(status, d.encoding == VR_PQ_RLE_DICTIONARY ? PQ_IDS_SHORT : PQ_PLAIN_SHORT, p);
+                } else if (d.encoding == VR_PQ_RLE_DICTIONARY) {
+                    v[j] = (uint32_t)compact[d.slot_base + r];
+                } else {
+                    const uint8_t* src = d.data + d.values_start + r * vb;
+                    uint64_t x = 0;
+                    for (int b = 0; b < vb; ++b) x |= (uint64_t)__ldg(src + b) << (8 * b);
+                    v[j] = x;
+                }
+            }
+            if (aligned && i0 + 4 <= n) {
+                if (vb == 4) {
+                    *reinterpret_cast<uint4*>(out + i0 * 4) =
+                        make_uint4((uint32_t)v[0], (uint32_t)v[1], (uint32_t)v[2], (uint32_t)v[3]);
+                } else {
+                    uint4* o = reinterpret_cast<uint4*>(out + i0 * 8);
+                    o[0] = make_uint4((uint32_t)v[0], (uint32_t)(v[0] >> 32), (uint32_t)v[1], (uint32_t)(v[1] >> 32));
+                    o[1] = make_uint4((uint32_t)v[2], (uint32_t)(v[2] >> 32), (uint32_t)v[3], (uint32_t)(v[3] >> 32));
+                }
             } else {
-                const uint8_t* src = d.data + d.values_start + r * vb;
-                for (int j = 0; j < vb; ++j) dst[j] = __ldg(src + j);
+                for (int j = 0; j < 4 && i0 + j < n; ++j)
+                    for (int b = 0; b < vb; ++b) out[(i0 + j) * vb + b] = (uint8_t)(v[j] >> (8 * b));
             }
         }
-        const uint32_t word = __ballot_sync(0xffffffffu, valid);
-        const int64_t wbase = i - lane;
-        if (lane == 0 && wbase < n) {
+        // the 32-slot validity word of lanes 8k..8k+7
+        uint32_t wv = nib << (4 * (lane & 7));
+        wv |= __shfl_xor_sync(0xffffffffu, wv, 1);
+        wv |= __shfl_xor_sync(0xffffffffu, wv, 2);
+        wv |= __shfl_xor_sync(0xffffffffu, wv, 4);
+        if ((lane & 7) == 0 && i0 < n) {
             if (validity) {
                 const int64_t nbytes = (n + 7) >> 3;
-                for (int j = 0; j < 4 && (wbase >> 3) + j < nbytes; ++j)
-                    validity[(wbase >> 3) + j] = (uint8_t)(word >> (8 * j));
+                for (int j = 0; j < 4 && (i0 >> 3) + j < nbytes; ++j) validity[(i0 >> 3) + j] = (uint8_t)(wv >> (8 * j));
             }
-            mine += __popc(word);
+            mine += __popc(wv);
         }
     }
+    for (int d = 16; d > 0; d >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, d);
     if (lane == 0 && mine) atomicAdd(&block_present, mine);
     __syncthreads();
     if (threadIdx.x == 0 && block_present)
@@ -924,8 +949,7 @@ int vr_pq_decode(vr_pq_decoder* d, int32_t num_pages, const vr_pq_page* pages, v
             const unsigned bx = (unsigned)std::min<int64_t>(64, std::max<int64_t>(1, (most + 8191) / 8192));
             for (int p0 = 0; p0 < num_pages && e == cudaSuccess; p0 += 65535) {
                 const unsigned np = (unsigned)std::min(65535, num_pages - p0);
-                k_pq_expand<<<dim3(bx, np, 2), 256, 0, st>>>(d->pages_dev, p0, d->runs, d->bits, d->compact,
-                                                              reinterpret_cast<int32_t*>(out_data));
+                k_pq_expand<<<dim3(bx, np, 2), 256, 0, st>>>(d->pages_dev, p0, d->runs, d->bits, d->compact);
                 e = cudaGetLastError();
             }
         }
