@@ -545,15 +545,85 @@ def run_e2e(args, w, lib, device):
 PQ_ROWS, PQ_PAGE_ROWS, PQ_DICT, PQ_NULLS = 60_000_000, 20_000, 100_000, 0.01
 
 
-def parquet_chunk(rows):
-    """A dictionary-encoded string column chunk: ids uniform over 100,000
-    entries (17-bit), 1% nulls, v1 data pages of 20,000 slots."""
+def parquet_ids(rows):
+    """The chunk's ids (uniform over 100,000 entries, 17-bit) and nulls (1%)."""
     from vecruntime_b200 import datagen as G
 
     rng = np.random.default_rng(G.SEEDS["parquet"])
     ids = rng.integers(0, PQ_DICT, size=rows).astype(np.int32)
     nulls = rng.random(rows) < PQ_NULLS
+    return ids, nulls
+
+
+def parquet_chunk(rows):
+    """A dictionary-encoded string column chunk: v1 RLE_DICTIONARY data pages
+    of 20,000 slots over `parquet_ids`."""
+    from vecruntime_b200 import datagen as G
+
+    ids, nulls = parquet_ids(rows)
     return G.dictionary_pages(ids, nulls, 17, PQ_PAGE_ROWS)
+
+
+def run_parquet_aggregate(args, out, valid, rows, device, check):
+    """The decoded column straight into the aggregate: count(*) grouped by
+    the string key, the chunk's 100,000-entry dictionary attached as a batch
+    dictionary (the aggregate maps it onto its table's once per batch). A
+    step resets the table and consumes the device-resident decoded column."""
+    import torch
+
+    import vecruntime_b200 as vr
+    from vecruntime_b200 import aggregate as A
+    from vecruntime_b200 import columns as Cc
+
+    words = [f"customer-{i:06d}" for i in range(PQ_DICT)]
+    dict_ = Cc.dictionary(words)
+    key = Cc.dict_strings(np.zeros(1, np.int32), dict_, np.zeros(1, bool), nullable=True)
+    db1, keep = Cc.to_device(Cc.HostBatch([key], 1), device)  # the dictionary in device memory
+    batch = Cc.DeviceBatch(rows, [out.data_ptr()], [valid.data_ptr()], dictionaries=db1.dictionaries)
+    from vecruntime_b200 import native as N
+
+    agg = vr.GpuHashAggregate([key], [0], [A.CountAgg()], est_groups=PQ_DICT + 1, max_batch_rows=rows,
+                              device=device, flags=N.VR_SPEC_TRACE)
+    stream = torch.cuda.ExternalStream(agg.stream(), device=torch.device("cuda", device))
+    times = []
+    k0 = 0.0
+    for it in range(args.warmup + args.steps):
+        if it == args.warmup:
+            k0 = agg.stats().total_kernel_ms
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        agg.reset()
+        agg.consume(batch)
+        b.record(stream)
+        agg.sync()
+        if it >= args.warmup:
+            times.append(a.elapsed_time(b))
+    kernel_ms = (agg.stats().total_kernel_ms - k0) / max(1, args.steps)
+    groups = agg.num_groups()
+    rec = {"ms_per_step": float(np.mean(times)), "rows/s": rows / (float(np.mean(times)) * 1e-3), "groups": groups,
+           "kernel_ms": kernel_ms,
+           "what": "count(*) group by the decoded string key (VR_DICT32 + batch dictionary), device-resident; "
+                   "the step includes the host's mapping of the 100,000-entry dictionary"}
+    if check:
+        got = agg.emit()
+        strings = agg.key_dictionary(0)
+        kd, kv = got[0]
+        cd = np.asarray(got[1][0])[:groups].astype(np.int64)
+        kvalid = Cc.unpack_bits(kv, groups)
+        ids, nulls = parquet_ids(rows)
+        want = np.bincount(ids[~nulls], minlength=PQ_DICT)
+        counts = np.zeros(PQ_DICT, np.int64)
+        null_count = 0
+        for g in range(groups):
+            if kvalid[g]:
+                counts[int(strings[int(kd[g])][len("customer-"):])] += cd[g]
+            else:
+                null_count += int(cd[g])
+        bad = int((counts != want).sum()) + int(null_count != int(nulls.sum()))
+        rec["parity"] = {"groups": groups, "want_groups": int((want > 0).sum()) + int(nulls.any()),
+                         "mismatches": bad, "rule": "per-string counts and the null group's count, exact"}
+    agg.close()
+    return rec
 
 
 def pq_pages_on(blob_ptr, pages):
@@ -658,6 +728,7 @@ def run_parquet(args, rank, world, device, check):
         "clocks": clocks.summary(),
         "parity": parity,
     }
+    rec["then_aggregate"] = run_parquet_aggregate(args, out, valid, rows, device, check)
     if not args.no_e2e:
         rec["e2e"] = run_parquet_e2e(args, dec, pages, blob, rows, device)
         rec["e2e"]["value"] = dist_min(rec["e2e"]["value"], world, device) * world
