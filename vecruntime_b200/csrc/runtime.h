@@ -4,8 +4,11 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cstring>
 #include <mutex>
 #include <string>
+#include <utility>
 #include <unordered_map>
 #include <vector>
 
@@ -62,10 +65,87 @@ struct StageSlot {
 // The strings of one VR_COL_BATCH_DICTIONARY key, in table-id order, and
 // their ids: every batch's dictionary is mapped onto it (GroupKeyTable's
 // StringDictionary, GroupKeyTable.java:1308-1430).
+// A table dictionary's string -> id map: open addressing over the strings'
+// bytes kept in one arena, so mapping a batch's dictionary (once per batch,
+// often right after a reset) allocates nothing per entry. It offers what the
+// batch mapping uses of a std::unordered_map: find / end / emplace / size /
+// clear, an entry reached as `it->second`, valid until the next emplace.
+class StrIdMap {
+public:
+    struct Entry {
+        int32_t second;
+    };
+    Entry* find(const std::string& s) {
+        if (slots_.empty()) return nullptr;
+        const uint64_t h = hash(s.data(), s.size());
+        for (size_t i = h & (slots_.size() - 1);; i = (i + 1) & (slots_.size() - 1)) {
+            const int32_t e = slots_[i];
+            if (e < 0) return nullptr;
+            if (hashes_[e] == h && len_[e] == s.size() && std::memcmp(arena_.data() + off_[e], s.data(), s.size()) == 0)
+                return &vals_[e];
+        }
+    }
+    Entry* end() { return nullptr; }
+    std::pair<Entry*, bool> emplace(const std::string& s, int32_t id) {
+        if (Entry* e = find(s)) return {e, false};
+        if (2 * (vals_.size() + 1) > slots_.size()) grow();
+        const uint64_t h = hash(s.data(), s.size());
+        const int32_t e = (int32_t)vals_.size();
+        off_.push_back(arena_.size());
+        len_.push_back(s.size());
+        hashes_.push_back(h);
+        vals_.push_back(Entry{id});
+        arena_.append(s);
+        size_t i = h & (slots_.size() - 1);
+        while (slots_[i] >= 0) i = (i + 1) & (slots_.size() - 1);
+        slots_[i] = e;
+        return {&vals_[e], true};
+    }
+    size_t size() const { return vals_.size(); }
+    void clear() {
+        std::fill(slots_.begin(), slots_.end(), -1);
+        arena_.clear();
+        off_.clear();
+        len_.clear();
+        hashes_.clear();
+        vals_.clear();
+    }
+
+private:
+    static uint64_t hash(const char* p, size_t n) {
+        uint64_t h = 0x9E3779B97F4A7C15ull ^ (n * 0xFF51AFD7ED558CCDull);
+        size_t i = 0;
+        for (; i + 8 <= n; i += 8) {
+            uint64_t w;
+            std::memcpy(&w, p + i, 8);
+            h = (h ^ w) * 0xC4CEB9FE1A85EC53ull;
+            h ^= h >> 29;
+        }
+        uint64_t t = 0;
+        std::memcpy(&t, p + i, n - i);
+        h = (h ^ t) * 0xC4CEB9FE1A85EC53ull;
+        return h ^ (h >> 32);
+    }
+    void grow() {
+        const size_t cap = slots_.empty() ? 1024 : 2 * slots_.size();
+        slots_.assign(cap, -1);
+        for (int32_t e = 0; e < (int32_t)vals_.size(); ++e) {
+            size_t i = hashes_[e] & (cap - 1);
+            while (slots_[i] >= 0) i = (i + 1) & (cap - 1);
+            slots_[i] = e;
+        }
+    }
+    std::vector<int32_t> slots_;
+    std::string arena_;
+    std::vector<size_t> off_, len_;
+    std::vector<uint64_t> hashes_;
+    std::vector<Entry> vals_;
+};
+
 struct TableDict {
     int key = -1;                  // key index in the spec
     int32_t limit = 0;             // the declared dict_size (0: no limit)
-    std::unordered_map<std::string, int32_t> ids;
+    StrIdMap ids;
     std::vector<int32_t> offsets{0};
     std::string bytes;
 };
